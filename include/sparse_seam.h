@@ -1,0 +1,183 @@
+/*
+ * sparse_seam.h -- C ABI of the B200-native exact dual regional-extrema route.
+ *
+ * Given an 8-bit grayscale image, the library writes two byte masks:
+ *   maxima[y][x] = 255 iff the 8-connected equal-valued flat zone of (x, y)
+ *                  has no strictly greater 8-neighbour, else 0;
+ *   minima[y][x] = 255 iff it has no strictly smaller 8-neighbour, else 0.
+ * Pixels outside the image are absent.  The masks are bit-exact against the
+ * reference's Sparse-Seam and Global-UF routes and against MATLAB
+ * imregionalmax / imregionalmin(img, 8).
+ *
+ * Everything crosses this boundary as plain pointers and sizes.  Device
+ * pointers are CUDA global-memory addresses of the current device; `stream`
+ * is a cudaStream_t passed as void* (NULL = the legacy default stream).
+ * No function throws.  The device entry points only enqueue work on the
+ * stream: they allocate nothing, never synchronise and may be captured into a
+ * CUDA graph.  One workspace serves one call in flight at a time; distinct
+ * workspaces on distinct streams may run concurrently from any host threads.
+ *
+ * Reference interfaces replaced (paths inside the reference repository):
+ *   ss_workspace_bytes   <- allocate_buffers sizing
+ *                           (harness/primary/snapshot_sparse_seam_cuda_v1_0.cu:710-737)
+ *                           and memory accounting
+ *                           (harness/primary/gpu_common_v0_6.cu:410-429)
+ *   ss_workspace_init    <- per-run cudaMemset of error_flag
+ *                           (harness/primary/gpu_common_v0_6.cu:147)
+ *   ss_extrema           <- run_sparse_resident
+ *                           (harness/primary/gpu_common_v0_6.cu:137-206)
+ *   ss_read_status       <- error_flag and tile_fragment_counts read-back
+ *                           (harness/primary/gpu_common_v0_6.cu:377-387,
+ *                            snapshot_sparse_seam_cuda_v1_0.cu:840-863)
+ *   ss_extrema_host      <- run_sparse_seam: H2D, kernels, D2H, kernel ms,
+ *                           active fragments
+ *                           (harness/primary/snapshot_sparse_seam_cuda_v1_0.cu:753-878)
+ *   ss_batch_*           <- the per-image host loop of the harness
+ *                           (harness/primary/gpu_common_v0_6.cu:584-745),
+ *                           replaced by one launch over many images.
+ */
+#ifndef SPARSE_SEAM_H
+#define SPARSE_SEAM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SS_ABI_VERSION 1
+
+typedef enum ss_status {
+    SS_OK = 0,
+    /* Host-side argument checks (nothing was enqueued). */
+    SS_ERR_INVALID_VALUE = 1,      /* NULL pointer, non-positive size, pitch < width */
+    SS_ERR_UNSUPPORTED_TILE = 2,   /* tile not in {16, 32, 64} */
+    SS_ERR_WORKSPACE_TOO_SMALL = 3,
+    SS_ERR_MISALIGNED = 4,         /* workspace / plan not 256-byte aligned */
+    SS_ERR_TOO_LARGE = 5,          /* beyond 32-bit pixel or fragment indexing */
+    SS_ERR_CUDA = 6,               /* a CUDA runtime call failed */
+    /* Device-side invariants, reported by ss_read_status. */
+    SS_ERR_FRAGMENT_OVERFLOW = 7,  /* a tile produced more seam fragments than
+                                      its slots (reference error_flag 1) */
+    SS_ERR_RECORD_RANGE = 8,       /* a fragment record out of range
+                                      (reference error_flag 2) */
+    SS_ERR_INVARIANT = 9,          /* a union-find link broke the min-root
+                                      order or left the arena (reference
+                                      error_flag 3) */
+    SS_ERR_SPIN_LIMIT = 10,        /* a bounded device loop gave up */
+    SS_ERR_WORKSPACE_UNINITIALIZED = 11, /* ss_workspace_init was not run */
+    SS_ERR_HOST_ALLOC = 12         /* host-side allocation failed */
+} ss_status;
+
+/* Human-readable name of a status code (static storage). */
+const char* ss_status_string(ss_status status);
+
+/* ABI version of the loaded library (SS_ABI_VERSION). */
+int ss_abi_version(void);
+
+/* Bytes of device workspace one call needs for a width x height image with
+ * the given tile size (16, 32 or 64).  The workspace holds the seam-fragment
+ * union-find arena (4*tile slots per tile), the per-tile border records, the
+ * per-tile fragment counts and seam-pair counters, and a status header. */
+ss_status ss_workspace_bytes(int width, int height, int tile, size_t* bytes);
+
+/* Resets a workspace (status header and seam-pair counters).  Required once
+ * after allocation, and again after any call whose status was not SS_OK. */
+ss_status ss_workspace_init(void* d_workspace, size_t workspace_bytes,
+                            void* stream);
+
+/* Enqueues the route for one device-resident image.
+ *   d_image    width x height bytes, rows `pitch` bytes apart (pitch >= width)
+ *   d_maxima,
+ *   d_minima   outputs, rows `out_pitch` bytes apart; 0/255 bytes
+ *   tile       16, 32 or 64: seam-fragment tile edge (the reference's SS_TILE)
+ * The masks do not depend on `tile`; only speed and the fragment statistics
+ * do.  Device-side invariant failures are recorded in the workspace header
+ * and returned by ss_read_status. */
+ss_status ss_extrema(const uint8_t* d_image, int width, int height, int pitch,
+                     int tile, uint8_t* d_maxima, uint8_t* d_minima,
+                     int out_pitch, void* d_workspace, size_t workspace_bytes,
+                     void* stream);
+
+typedef struct ss_stats {
+    uint32_t device_error;        /* ss_status of the first device invariant
+                                     failure since the last read, or 0 */
+    uint32_t error_detail;        /* implementation detail of that failure */
+    uint64_t active_fragments;    /* seam fragments of the last call
+                                     (sum of per-tile counts) */
+    uint64_t tiles;               /* tiles of the last call */
+    uint64_t flipped_tiles;       /* tiles whose seam fragments changed
+                                     verdict after the global merge */
+} ss_stats;
+
+/* Synchronises `stream`, copies the status header (and, if `stats` is not
+ * NULL, the statistics) to the host and clears the device error word.
+ * Returns SS_OK or the first device-side failure. */
+ss_status ss_read_status(void* d_workspace, size_t workspace_bytes,
+                         void* stream, ss_stats* stats);
+
+/* Host-to-host convenience form: copies a host image to the device, runs
+ * ss_extrema, copies both masks back and synchronises.  Device buffers and
+ * pinned staging are owned by an opaque context so repeated calls reuse them.
+ * `elapsed_ms` (optional) receives the device time of the kernels alone;
+ * `active_fragments` (optional) the fragment count. */
+typedef struct ss_context ss_context;
+ss_status ss_context_create(int device, ss_context** context);
+void ss_context_destroy(ss_context* context);
+ss_status ss_extrema_host(ss_context* context, const uint8_t* h_image,
+                          int width, int height, int pitch, int tile,
+                          uint8_t* h_maxima, uint8_t* h_minima, int out_pitch,
+                          float* elapsed_ms, uint64_t* active_fragments);
+
+/* ---------------------------------------------------------------------- */
+/* Batches: many images of uneven sizes in one launch pair.                */
+/* ---------------------------------------------------------------------- */
+
+typedef struct ss_image_desc {
+    const uint8_t* image;   /* device pointer */
+    uint8_t* maxima;        /* device pointer */
+    uint8_t* minima;        /* device pointer */
+    int32_t width;
+    int32_t height;
+    int32_t pitch;
+    int32_t out_pitch;
+} ss_image_desc;
+
+/* Size of the device plan for `count` images and `total_tiles` tiles (the
+ * sum over images of ceil(w/tile)*ceil(h/tile); pass 0 to have it computed
+ * by ss_batch_plan_fill). */
+ss_status ss_batch_plan_bytes(int count, int64_t total_tiles, size_t* bytes);
+
+/* Counts the tiles of a batch for a given tile size. */
+ss_status ss_batch_tiles(const ss_image_desc* descs, int count, int tile,
+                         int64_t* total_tiles);
+
+/* Fills a HOST buffer with the plan (image table, tile offsets and the
+ * tile-to-image map) for `descs`.  The caller copies it to a 256-byte aligned
+ * device buffer of the same size (e.g. cudaMemcpyAsync) before
+ * ss_extrema_batch; a plan stays valid for as long as the images' pointers
+ * and sizes do, so it can be reused across calls and graph replays.
+ * `workspace_bytes` (optional) receives the workspace size the batch needs. */
+ss_status ss_batch_plan_fill(const ss_image_desc* descs, int count, int tile,
+                             void* h_plan, size_t plan_bytes,
+                             size_t* workspace_bytes);
+
+/* Enqueues the route over every image of a plan.  `h_plan` is the host plan
+ * filled by ss_batch_plan_fill (read for sizes only), `d_plan` its device
+ * copy (read by the kernels).  Each image gets its own seam-fragment arena
+ * inside the workspace; results are the same as calling ss_extrema on each
+ * image alone.
+ *   persistent  0: one CTA per (image, tile) work item;
+ *               1: a persistent grid (one wave of CTAs) that pops
+ *                  (image, tile) items from a device work queue. */
+ss_status ss_extrema_batch(const void* h_plan, const void* d_plan,
+                           size_t plan_bytes, int persistent,
+                           void* d_workspace, size_t workspace_bytes,
+                           void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPARSE_SEAM_H */

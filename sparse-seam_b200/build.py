@@ -1,0 +1,63 @@
+"""Build recipe for the CUDA route library (sm_100a).
+
+Compiles ``csrc/ss_route.cu`` into ``libsparseseam.so`` next to this file with
+nvcc.  The library has a plain C ABI (``include/sparse_seam.h``) and links the
+CUDA runtime statically, so it loads into any process on the GPU host, with or
+without PyTorch.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+INCLUDE = os.path.join(ROOT, "include")
+SOURCES = [os.path.join(HERE, "csrc", "ss_route.cu")]
+DEPENDS = SOURCES + [
+    os.path.join(HERE, "csrc", "ss_device.cuh"),
+    os.path.join(HERE, "csrc", "ss_tile.cuh"),
+    os.path.join(INCLUDE, "sparse_seam.h"),
+]
+LIBRARY = os.path.join(HERE, "libsparseseam.so")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc",
+                 shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def command(output: str, extra=()) -> list:
+    return [
+        nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17",
+        "-I" + INCLUDE, "-Xcompiler", "-fPIC", "-shared",
+        "-Xptxas", "-warn-spills",
+        *extra, "-o", output, *SOURCES,
+    ]
+
+
+def stale() -> bool:
+    if not os.path.exists(LIBRARY):
+        return True
+    built = os.path.getmtime(LIBRARY)
+    return any(os.path.getmtime(d) > built for d in DEPENDS)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not stale():
+        return LIBRARY
+    tmp = LIBRARY + ".tmp"
+    extra = ["-Xptxas", "-v"] if verbose else []
+    subprocess.check_call(command(tmp, extra))
+    os.replace(tmp, LIBRARY)
+    return LIBRARY
+
+
+if __name__ == "__main__":
+    import sys
+    print(build(force=True, verbose="-v" in sys.argv))

@@ -1,0 +1,181 @@
+"""Bit-exact parity of the CUDA route with the CPU oracle and the golden masks.
+
+Every test here calls the sm_100a library through its C ABI (via the package's
+ctypes binding).  Masks are bytes, so the bar is exact equality.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import package
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TILES = (16, 32, 64)
+
+
+def run_gpu(image: np.ndarray, tile: int, pitch_pad: int = 0,
+            out_pad: int = 0, ws=None):
+    pkg = package()
+    h, w = image.shape
+    dev = torch.device("cuda")
+    if pitch_pad:
+        buf = torch.full((h, w + pitch_pad), 77, dtype=torch.uint8, device=dev)
+        buf[:, :w] = torch.from_numpy(image).to(dev)
+        d_img = buf[:, :w]
+    else:
+        d_img = torch.from_numpy(np.ascontiguousarray(image)).to(dev)
+    if out_pad:
+        mxb = torch.full((h, w + out_pad), 9, dtype=torch.uint8, device=dev)
+        mnb = torch.full((h, w + out_pad), 9, dtype=torch.uint8, device=dev)
+        mx, mn = mxb[:, :w], mnb[:, :w]
+    else:
+        mx = mn = None
+    mx, mn = pkg.extrema(d_img, tile=tile, maxima=mx, minima=mn,
+                         workspace=ws)
+    torch.cuda.synchronize()
+    out = (mx.cpu().numpy(), mn.cpu().numpy())
+    if out_pad:
+        assert (mxb[:, w:] == 9).all() and (mnb[:, w:] == 9).all(), \
+            "wrote outside the output rows"
+    return out
+
+
+def assert_same(got, want, what):
+    gmx, gmn = got
+    wmx, wmn = want
+    if not np.array_equal(gmx, wmx) or not np.array_equal(gmn, wmn):
+        raise AssertionError(
+            f"{what}: {int((gmx != wmx).sum())} maxima and "
+            f"{int((gmn != wmn).sum())} minima pixels differ")
+
+
+@pytest.mark.parametrize("tile", TILES)
+def test_golden_cases(golden_cases, tile):
+    pkg = package()
+    for c in golden_cases:
+        h, w = c.image.shape
+        ws = pkg.Workspace.for_image(w, h, tile)
+        got = run_gpu(c.image, tile, ws=ws)
+        stats = ws.read_status()
+        assert_same(got, (c.maxima, c.minima), f"{c} T={tile}")
+        assert int((got[0] != 0).sum()) == c.manifest_max
+        assert int((got[1] != 0).sum()) == c.manifest_min
+        frag = int(oracle.tile_fragments(c.image, tile).sum())
+        assert stats.active_fragments == frag, (c, tile)
+
+
+@pytest.mark.parametrize("tile", TILES)
+def test_random_images_against_oracle(tile):
+    rng = np.random.default_rng(1000 + tile)
+    for trial in range(40):
+        h = int(rng.integers(1, 300))
+        w = int(rng.integers(1, 300))
+        levels = int(rng.choice([2, 3, 4, 8, 16, 64, 256]))
+        img = rng.integers(0, levels, size=(h, w)).astype(np.uint8)
+        got = run_gpu(img, tile, pitch_pad=int(rng.integers(0, 3)) * 13,
+                      out_pad=int(rng.integers(0, 2)) * 5)
+        assert_same(got, oracle.extrema(img), f"trial {trial} {h}x{w} q{levels}")
+
+
+def test_config1_uniform_q16_and_constant():
+    synth = pytest.importorskip("importlib").import_module(
+        "sparse-seam_b200.synth")
+    for img in (synth.uniform_q16(512, 512, 0), synth.constant(512, 512, 128)):
+        want = oracle.extrema(img)
+        for tile in TILES:
+            assert_same(run_gpu(img, tile), want, f"config1 T={tile}")
+    c = synth.constant(512, 512, 128)
+    got = run_gpu(c, 32)
+    assert (got[0] == 255).all() and (got[1] == 255).all()
+
+
+def test_plateau_and_seam_heavy_families():
+    import importlib
+    synth = importlib.import_module("sparse-seam_b200.synth")
+    imgs = {
+        "ellipse_edt": synth.ellipse_edt(1024, 1024, 3),
+        "serpentine": synth.serpentine(1024, 1024),
+        "spiral": synth.spiral(1024, 1024),
+        "blocks": synth.blocks(1024, 1024, 8, 0, 5),
+        "blocks_shift16": synth.blocks(1024, 1024, 8, 16, 5),
+        "checker1": synth.checkerboard(1024, 1024, 1),
+        "checker3": synth.checkerboard(1024, 1024, 3),
+        "checker17": synth.checkerboard(1024, 1024, 17),
+    }
+    for name, img in imgs.items():
+        want = oracle.extrema(img)
+        for tile in TILES:
+            assert_same(run_gpu(img, tile), want, f"{name} T={tile}")
+
+
+def test_smooth_noise_quantization_sweep_full_size():
+    import importlib
+    synth = importlib.import_module("sparse-seam_b200.synth")
+    base = synth.smooth_noise(1356, 2040, seed=11, device="cuda").cpu().numpy()
+    for levels in (256, 64, 16, 4, 2):
+        img = synth.quantize(base, levels)
+        want = oracle.extrema(img, method="bands", threads=8)
+        for tile in TILES:
+            assert_same(run_gpu(img, tile), want, f"smooth q{levels} T={tile}")
+
+
+def test_repeatable_and_workspace_reuse_across_geometries():
+    pkg = package()
+    rng = np.random.default_rng(5)
+    ws = pkg.Workspace(pkg.workspace_bytes(700, 700, 16))
+    imgs = [rng.integers(0, 4, size=s).astype(np.uint8)
+            for s in [(700, 700), (33, 650), (512, 97), (700, 700)]]
+    for rep in range(3):
+        for img in imgs:
+            for tile in TILES:
+                got = run_gpu(img, tile, ws=ws)
+                ws.read_status()
+                assert_same(got, oracle.extrema(img), f"rep {rep} T={tile}")
+
+
+@pytest.mark.parametrize("persistent", [False, True])
+@pytest.mark.parametrize("tile", TILES)
+def test_batch_equals_single(persistent, tile):
+    import importlib
+    pkg = package()
+    synth = importlib.import_module("sparse-seam_b200.synth")
+    images = synth.uneven_batch(48, seed=tile, lo=16, hi=400, device="cuda")
+    maxs, mins = pkg.extrema_batch(images, tile=tile, persistent=persistent)
+    for i, im in enumerate(images):
+        host = im.cpu().numpy()
+        want = oracle.extrema(host)
+        assert_same((maxs[i].cpu().numpy(), mins[i].cpu().numpy()), want,
+                    f"batch image {i} {host.shape}")
+
+
+def test_batch_replay_is_stable():
+    import importlib
+    pkg = package()
+    synth = importlib.import_module("sparse-seam_b200.synth")
+    images = synth.uneven_batch(32, seed=9, lo=64, hi=512, device="cuda")
+    maxs = [torch.empty_like(i) for i in images]
+    mins = [torch.empty_like(i) for i in images]
+    plan = pkg.BatchPlan(images, maxs, mins, tile=32)
+    ws = plan.make_workspace()
+    plan.run(ws, persistent=True)
+    ws.read_status()
+    first = [(a.clone(), b.clone()) for a, b in zip(maxs, mins)]
+    for rep in range(5):
+        for m in maxs + mins:
+            m.fill_(3)
+        plan.run(ws, persistent=bool(rep % 2))
+        ws.read_status()
+        for (a, b), mx, mn in zip(first, maxs, mins):
+            assert torch.equal(a, mx) and torch.equal(b, mn)
+
+
+def test_uninitialized_workspace_is_reported():
+    pkg = package()
+    img = torch.zeros((64, 64), dtype=torch.uint8, device="cuda")
+    ws = pkg.Workspace(pkg.workspace_bytes(64, 64, 32))
+    ws.buffer.zero_()  # wipes the header written by init
+    with pytest.raises(pkg.SparseSeamError) as e:
+        pkg.extrema(img, tile=32, workspace=ws, check=True)
+    assert e.value.status == 11
