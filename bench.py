@@ -1,0 +1,629 @@
+#!/usr/bin/env python
+"""Benchmark: exact dual regional-extrema masks (bit-exact), Gpix/s.
+
+Workload (one "step"): the natural-image-like corpus -- 100 images of
+2040x1356 plus 100 of 481x321 uint8 smooth noise (sigma 1/4/16 px fields,
+weights 0.2/0.3/0.5, U{-2..2} jitter), tile T = 32, all 256 gray levels.
+292.5 Mpix per step; inputs (292 MB) plus masks (585 MB) exceed the 126 MB
+L2, so no L2 flush is needed between steps.
+
+  value        whole-job Gpix/s of the batched form: both passes of the route
+               over the whole corpus in one launch pair, replayed from a CUDA
+               graph, inputs already resident in HBM, timed with CUDA events
+               (max over ranks)
+  e2e          the same metric through the public host-to-host API (pinned
+               host images -> device -> both masks back to pinned host
+               memory, chunked so copies overlap the kernels)
+  per_image    the plain per-image launch (one ss_extrema per image, graph
+               replayed) -- the form the batched path must beat
+  roofline     the tile pass (dominant kernel) against the 3 B/pixel
+               compulsory traffic (1 B read + 2 B written) at the measured
+               HBM copy bandwidth
+  cpu_baseline the CPU union-find oracle over the same corpus on the host's
+               cores (one image per thread)
+  reference_gpu  the reference's own Sparse-Seam v1.0 and Global-UF routes,
+               compiled unchanged for sm_100a, per-image protocol of the
+               reference harness (median of reps), on a sample of the corpus
+
+--impl reference times the CPU exact path (the reference has no CPU
+implementation of this route; the oracle port stands in) on the same corpus.
+
+Multi-GPU: one process per GPU (torchrun); every rank processes its own
+corpus (replicas, weak scaling); no collective touches the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Gpix/s dual masks (bit-exact), batched vs per-image; p50/p99 served latency"
+UNIT = "Gpix/s"
+BYTES_PER_PIXEL = 3  # 1 B image read + 2 B mask writes
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="sparse-seam-b200",
+                   choices=["sparse-seam-b200", "reference"])
+    p.add_argument("--tile", type=int, default=32)
+    p.add_argument("--large", type=int, default=100)
+    p.add_argument("--small", type=int, default=100)
+    p.add_argument("--quick", action="store_true",
+                   help="skip the secondary measurements (per-image, e2e, "
+                        "CPU baseline, reference GPU routes)")
+    p.add_argument("--passes-only", action="store_true",
+                   help="only run the split-pass loop (for profiling)")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# Distributed plumbing (one process per GPU)
+# ---------------------------------------------------------------------------
+
+class Dist:
+    def __init__(self):
+        import torch
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group(
+                "nccl", timeout=datetime.timedelta(seconds=300),
+                device_id=torch.device("cuda", self.local))
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            import torch.distributed as dist
+            dist.barrier(device_ids=[self.local])
+            torch.cuda.synchronize()
+
+    def max(self, value: float) -> float:
+        if not self.pg:
+            return value
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([value], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region
+# ---------------------------------------------------------------------------
+
+REASONS = [
+    ("hw_slowdown", "clocks_event_reasons.hw_slowdown"),
+    ("hw_thermal_slowdown", "clocks_event_reasons.hw_thermal_slowdown"),
+    ("sw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown"),
+    ("sw_power_cap", "clocks_event_reasons.sw_power_cap"),
+]
+
+
+class ClockSampler:
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+        self._thread = None
+
+    def start(self):
+        fields = ["index", "clocks.sm", "clocks.max.sm", "power.draw"] + \
+            [q for _, q in REASONS]
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={','.join(fields)}",
+                 "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device_index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self._thread = threading.Thread(target=self._read, daemon=True)
+        self._thread.start()
+        time.sleep(0.3)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "note": "nvidia-smi unavailable"}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._thread:
+            self._thread.join(timeout=2)
+        sm, smax, power = [], [], []
+        active = set()
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 4 + len(REASONS):
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for (name, _), val in zip(REASONS, parts[4:]):
+                if val.lower().startswith("active"):
+                    active.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "power_w_max": max(power), "reasons": sorted(active),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# Workload
+# ---------------------------------------------------------------------------
+
+def corpus_shapes(n_large: int, n_small: int):
+    return [(1356, 2040)] * n_large + [(321, 481)] * n_small
+
+
+def make_corpus(n_large: int, n_small: int, seed_base: int, device):
+    from importlib import import_module
+    synth = import_module("sparse-seam_b200.synth")
+    return [synth.smooth_noise(h, w, seed_base + i, device=device)
+            for i, (h, w) in enumerate(corpus_shapes(n_large, n_small))]
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            data = json.load(f)
+        return float(data["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """DRAM bytes per pixel of the tile pass from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "tile_pass_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# CPU exact path (reference arm and cpu_baseline)
+# ---------------------------------------------------------------------------
+
+def time_cpu_oracle(host_images, threads: int, reps: int = 1):
+    import oracle
+    pixels = sum(im.size for im in host_images)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        oracle.extrema_batch(host_images, threads=threads)
+        times.append(time.perf_counter() - t0)
+    return pixels, times
+
+
+def run_reference_arm(args, dist: Dist):
+    import torch
+    if dist.rank != 0:
+        return 0
+    device = "cuda" if torch.cuda.is_available() else "cpu"
+    images = [t.cpu().numpy() for t in
+              make_corpus(args.large, args.small, 0, device)]
+    threads = cpu_threads()
+    pixels, _ = time_cpu_oracle(images, threads, reps=max(1, args.warmup))
+    _, times = time_cpu_oracle(images, threads, reps=args.steps)
+    total = sum(times)
+    value = pixels * args.steps / total / 1e9
+    sample = (f"the full corpus per step ({args.large} x 2040x1356 + "
+              f"{args.small} x 481x321, {pixels} px), union-find oracle, "
+              f"one image per thread")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 6),
+        "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "synthetic (seeded smooth-noise corpus)",
+        "config": config_dict(args),
+        "cpu_baseline": {"value": round(value, 6), "unit": UNIT,
+                         "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": round(value, 6), "unit": UNIT,
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": ("the reference ships no CPU implementation of the route; "
+                 "the C restatement of its rule (oracle/ss_oracle.c) is timed"),
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def config_dict(args):
+    return {
+        "workload": (f"natural-image-like corpus: {args.large} x 2040x1356 + "
+                     f"{args.small} x 481x321 uint8 smooth noise, 256 levels"),
+        "tile": args.tile,
+        "images_per_step": args.large + args.small,
+        "pixels_per_step": sum(h * w for h, w in
+                               corpus_shapes(args.large, args.small)),
+        "l2": "inputs + masks (877 MB) exceed L2; no flush",
+        "parallelism": f"replicas x{args.gpus}",
+    }
+
+
+# ---------------------------------------------------------------------------
+# Reference GPU routes (checker build, oracle/_ref)
+# ---------------------------------------------------------------------------
+
+def reference_gpu_routes(host_images, tile: int, warmup=3, reps=10):
+    path = os.path.join(ROOT, "oracle", "_ref", f"libssref_t{tile}.so")
+    if not os.path.exists(path):
+        return {"unavailable": f"{os.path.relpath(path, ROOT)} not built"}
+    import numpy as np
+    lib = ctypes.CDLL(path)
+    u8 = ctypes.POINTER(ctypes.c_uint8)
+    d = ctypes.POINTER(ctypes.c_double)
+    lib.ssref_sparse_seam.argtypes = [u8, ctypes.c_int, ctypes.c_int, u8, u8,
+                                      ctypes.c_int, ctypes.c_int, d, d,
+                                      ctypes.POINTER(ctypes.c_longlong)]
+    lib.ssref_global_uf.argtypes = [u8, ctypes.c_int, ctypes.c_int, u8, u8,
+                                    ctypes.c_int, ctypes.c_int, d, d]
+    out = {}
+    for name in ("sparse_seam_v1_0", "global_uf"):
+        pix = 0
+        sec = 0.0
+        h2h = 0.0
+        for img in host_images:
+            h, w = img.shape
+            img = np.ascontiguousarray(img)
+            mx = np.empty_like(img)
+            mn = np.empty_like(img)
+            ms = ctypes.c_double()
+            hms = ctypes.c_double()
+            if name == "sparse_seam_v1_0":
+                frag = ctypes.c_longlong()
+                rc = lib.ssref_sparse_seam(
+                    img.ctypes.data_as(u8), w, h, mx.ctypes.data_as(u8),
+                    mn.ctypes.data_as(u8), warmup, reps, ctypes.byref(ms),
+                    ctypes.byref(hms), ctypes.byref(frag))
+            else:
+                rc = lib.ssref_global_uf(
+                    img.ctypes.data_as(u8), w, h, mx.ctypes.data_as(u8),
+                    mn.ctypes.data_as(u8), warmup, reps, ctypes.byref(ms),
+                    ctypes.byref(hms))
+            if rc != 0:
+                out[name] = {"error": "reference route raised"}
+                break
+            pix += img.size
+            sec += ms.value / 1e3
+            h2h += hms.value / 1e3
+        else:
+            out[name] = {"value": round(pix / sec / 1e9, 4), "unit": UNIT,
+                         "h2h_value": round(pix / h2h / 1e9, 4),
+                         "protocol": (f"per image: {warmup} warm-ups, median "
+                                      f"of {reps} reps; sum(px)/sum(median)")}
+    out["sample"] = f"{len(host_images)} images of the corpus"
+    out["tile"] = tile
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Product arm
+# ---------------------------------------------------------------------------
+
+def main():
+    args = parse_args()
+    import torch
+    dist = Dist()
+    if args.impl == "reference":
+        rc = run_reference_arm(args, dist)
+        dist.close()
+        return rc
+    from importlib import import_module
+    pkg = import_module("sparse-seam_b200")
+    device = torch.device("cuda", dist.local)
+    torch.cuda.set_device(device)
+    tile = args.tile
+
+    images = make_corpus(args.large, args.small, 7919 * dist.rank, device)
+    pixels = sum(im.numel() for im in images)
+    maxs = [torch.empty_like(im) for im in images]
+    mins = [torch.empty_like(im) for im in images]
+    plan = pkg.BatchPlan(images, maxs, mins, tile=tile)
+    ws = plan.make_workspace()
+    stream = torch.cuda.Stream(device)
+    torch.cuda.synchronize()
+
+    # -- correctness of this very workload (outside every timed region) ---
+    plan.run(ws, persistent=False, stream=stream)
+    stats = ws.read_status(stream)
+    host_images = [im.cpu().numpy() for im in images]
+    import numpy as np
+    import oracle
+    check_n = len(images) if dist.rank == 0 else 4
+    idx = list(range(0, len(images), max(1, len(images) // check_n)))[:check_n]
+    want_max, want_min = oracle.extrema_batch([host_images[i] for i in idx],
+                                              threads=cpu_threads())
+    mismatches = 0
+    for j, i in enumerate(idx):
+        mismatches += int((maxs[i].cpu().numpy() != want_max[j]).sum())
+        mismatches += int((mins[i].cpu().numpy() != want_min[j]).sum())
+    if mismatches:
+        print(json.dumps({"error": "masks differ from the oracle",
+                          "mismatched_pixels": mismatches}))
+        return 1
+
+    if args.passes_only:
+        for _ in range(max(1, args.steps)):
+            plan.run_pass(ws, 1, stream=stream)
+            plan.run_pass(ws, 2, stream=stream)
+        ws.read_status(stream)
+        return 0
+
+    # -- schedule: one CTA per work item vs the persistent work queue -------
+    def timed(fn, reps):
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(reps):
+            fn()
+        e.record(stream)
+        e.synchronize()
+        return s.elapsed_time(e) / reps
+
+    sched = {}
+    for persistent in (False, True):
+        timed(lambda: plan.run(ws, persistent=persistent, stream=stream), 2)
+        sched[persistent] = timed(
+            lambda: plan.run(ws, persistent=persistent, stream=stream), 3)
+    persistent = sched[True] < sched[False]
+    ws.read_status(stream)
+
+    # -- batched form, graph-replayed: the headline value ------------------
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(stream):
+        plan.run(ws, persistent=persistent, stream=stream)  # warm capture path
+        stream.synchronize()
+        with torch.cuda.graph(graph, stream=stream):
+            plan.run(ws, persistent=persistent, stream=stream)
+    for _ in range(args.warmup):
+        graph.replay()
+    stream.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        for _ in range(args.steps):
+            graph.replay()
+        ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    dist.barrier()
+    ms_local = ev0.elapsed_time(ev1)
+    ms_total = dist.max(ms_local)
+    value = dist.world * pixels * args.steps / (ms_total / 1e3) / 1e9
+    stats = ws.read_status(stream)
+
+    # -- per-pass timing (roofline of the tile pass) ----------------------
+    s1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    s2 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    t_pass1 = []
+    t_pass2 = []
+    for k in range(args.steps):
+        s1[k].record(stream)
+        plan.run_pass(ws, 1, persistent=persistent, stream=stream)
+        s2[k].record(stream)
+        plan.run_pass(ws, 2, persistent=persistent, stream=stream)
+        s1[k + 1].record(stream)
+    stream.synchronize()
+    for k in range(args.steps):
+        t_pass1.append(s1[k].elapsed_time(s2[k]))
+        t_pass2.append(s2[k].elapsed_time(s1[k + 1]))
+    ws.read_status(stream)
+    tile_ms = statistics.mean(t_pass1)
+    resolve_ms = statistics.mean(t_pass2)
+    hbm, peak_kind = peaks()
+    achieved = BYTES_PER_PIXEL * pixels / (tile_ms / 1e3) / 1e9
+    traffic = committed_traffic()
+    traffic_bytes = None
+    if traffic and traffic.get("tile") == tile:
+        traffic_bytes = int(traffic["dram_bytes_per_pixel"] * pixels)
+
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT,
+        "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_total / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "synthetic (seeded smooth-noise corpus)",
+        "config": config_dict(args),
+        "schedule": {"persistent": persistent,
+                     "ms_grid": round(sched[False], 4),
+                     "ms_persistent": round(sched[True], 4)},
+        "gpu_launches": 2 * args.steps,
+        "passes_ms": {"tile_pass": round(tile_ms, 4),
+                      "resolve_pass": round(resolve_ms, 4)},
+        "roofline": {"bound": "hbm", "kernel": "tile_pass_kernel",
+                     "achieved": round(achieved, 2), "peak": hbm,
+                     "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4),
+                     "traffic": traffic_bytes,
+                     "algorithmic_bytes": BYTES_PER_PIXEL * pixels},
+        "route_roofline_frac": round(
+            BYTES_PER_PIXEL * pixels / (ms_total / args.steps / 1e3) / 1e9
+            / hbm, 4),
+        "stats": {"active_fragments": int(stats.active_fragments),
+                  "tiles": int(stats.tiles),
+                  "flipped_tiles_per_step": None},
+        "clocks": clock_info,
+        "checked_images": len(idx),
+        "mismatches": mismatches,
+    }
+
+    if not args.quick:
+        line.update(secondary(args, pkg, plan, images, host_images, maxs,
+                              mins, stream, dist, hbm))
+    elif dist.rank == 0:
+        line["cpu_baseline"] = None
+        line["e2e"] = None
+
+    del graph
+    if dist.rank == 0:
+        print(json.dumps(line))
+    dist.close()
+    return 0
+
+
+def secondary(args, pkg, plan, images, host_images, maxs, mins, stream, dist,
+              hbm):
+    import torch
+    out = {}
+    tile = args.tile
+    pixels = sum(im.numel() for im in images)
+
+    # -- plain per-image launches, graph-replayed ----------------------------
+    big = max(images, key=lambda t: t.numel())
+    ws1 = pkg.Workspace.for_image(big.shape[1], big.shape[0], tile)
+
+    def per_image_graph(sel):
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(stream):
+            for i in sel:
+                pkg.extrema(images[i], tile, maxs[i], mins[i], ws1,
+                            stream=stream)
+            stream.synchronize()
+            with torch.cuda.graph(g, stream=stream):
+                for i in sel:
+                    pkg.extrema(images[i], tile, maxs[i], mins[i], ws1,
+                                stream=stream)
+        for _ in range(args.warmup):
+            g.replay()
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(args.steps):
+                g.replay()
+            e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        del g
+        return ms
+
+    all_ms = per_image_graph(range(len(images)))
+    large = [i for i, t in enumerate(images) if t.shape == (1356, 2040)]
+    large_ms = per_image_graph(large) if large else None
+    ws1.read_status(stream)
+    out["per_image"] = {
+        "value": round(pixels / (all_ms / 1e3) / 1e9, 4), "unit": UNIT,
+        "ms_per_step": round(all_ms, 4),
+        "launches_per_image": 2,
+    }
+    if large_ms:
+        px = 2040 * 1356
+        per = large_ms / len(large)
+        out["single_image_2040x1356"] = {
+            "us_per_image": round(per * 1e3, 3),
+            "gpix_s": round(px / (per / 1e3) / 1e9, 4),
+            "roofline_frac": round(BYTES_PER_PIXEL * px / (per / 1e3) / 1e9
+                                   / hbm, 4),
+            "protocol": ("graph of one ss_extrema per image over the "
+                         f"{len(large)} distinct 2040x1356 images, replayed "
+                         "back to back"),
+        }
+
+    # -- e2e: host-to-host through the public API ---------------------------
+    host = __import__("importlib").import_module("sparse-seam_b200.host")
+    hb = host.HostBatch(host_images, tile=tile, chunks=8,
+                        persistent=False)
+    for _ in range(args.warmup):
+        hb.run(stream)
+    stream.synchronize()
+    hb.check()
+    dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    end = None
+    for _ in range(args.steps):
+        end = hb.run(stream)
+    end.synchronize()
+    e2e_ms = dist.max(e0.elapsed_time(end))
+    hb.check()
+    import numpy as np
+    bad = sum(int((hb.maxima[i] != maxs[i].cpu().numpy()).sum()) +
+              int((hb.minima[i] != mins[i].cpu().numpy()).sum())
+              for i in range(0, len(images), 25))
+    out["e2e"] = {
+        "value": round(dist.world * pixels * args.steps / (e2e_ms / 1e3)
+                       / 1e9, 4),
+        "unit": UNIT, "h2d_bytes_per_step": hb.h2d_bytes,
+        "d2h_bytes_per_step": hb.d2h_bytes,
+        "ms_per_step": round(e2e_ms / args.steps, 3),
+        "api": "sparse-seam_b200.host.HostBatch (ss_extrema_batch, 8 chunks)",
+        "mismatches_vs_device_run": bad,
+    }
+
+    # -- CPU exact path on the host's cores (rank 0, N=1 only) -------------
+    if dist.rank == 0 and dist.world == 1:
+        threads = cpu_threads()
+        cpix, ctimes = time_cpu_oracle(host_images, threads, reps=2)
+        cval = cpix / min(ctimes) / 1e9
+        out["cpu_baseline"] = {
+            "value": round(cval, 5), "unit": UNIT, "cores": threads,
+            "kind": "port",
+            "sample": (f"the whole corpus ({cpix} px), union-find oracle "
+                       "(oracle/ss_oracle.c), one image per thread, best "
+                       "of 2"),
+        }
+        sample = [host_images[i] for i in (0, 1, 2, 3, 4)] + \
+            [host_images[i] for i in range(len(images) - 5, len(images))]
+        out["reference_gpu"] = reference_gpu_routes(sample, tile)
+    return out
+
+
+if __name__ == "__main__":
+    sys.exit(main())

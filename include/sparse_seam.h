@@ -104,12 +104,29 @@ typedef struct ss_stats {
     uint32_t device_error;        /* ss_status of the first device invariant
                                      failure since the last read, or 0 */
     uint32_t error_detail;        /* implementation detail of that failure */
-    uint64_t active_fragments;    /* seam fragments of the last call
-                                     (sum of per-tile counts) */
+    uint64_t active_fragments;    /* seam fragments of the last call (sum
+                                     of per-tile counts).  The CTA-per-tile
+                                     kernels create one per seam-touching
+                                     tile-local zone, exactly the reference's
+                                     tile_fragment_counts; the row-scan
+                                     kernels only one per seam zone whose
+                                     verdict the merge can still change */
     uint64_t tiles;               /* tiles of the last call */
     uint64_t flipped_tiles;       /* tiles whose seam fragments changed
                                      verdict after the global merge */
 } ss_stats;
+
+/* Kernel configuration used for a tile size by every later call of this
+ * process (the autotuner's hook; the masks never depend on it).
+ *   warps > 0   CTA-per-tile kernels with `warps` warps per CTA
+ *               (tile 16: 2, 4 or 8; tile 32: 4, 8 or 16; tile 64: 8 or 16)
+ *   warps < 0   tile 32 only: row-scan kernels, one tile per warp, -warps
+ *               warps per CTA (2 or 4)
+ * Defaults: tile 16 -> 4, tile 32 -> -4, tile 64 -> 16.  The reference fixes
+ * its tile and classify threads at compile time
+ * (harness/configuration_study/sparse_config_benchmark_v0_8.cu:17-30). */
+ss_status ss_set_kernel_config(int tile, int warps);
+ss_status ss_get_kernel_config(int tile, int* warps);
 
 /* Synchronises `stream`, copies the status header (and, if `stats` is not
  * NULL, the statistics) to the host and clears the device error word.
@@ -118,8 +135,8 @@ ss_status ss_read_status(void* d_workspace, size_t workspace_bytes,
                          void* stream, ss_stats* stats);
 
 /* Host-to-host convenience form: copies a host image to the device, runs
- * ss_extrema, copies both masks back and synchronises.  Device buffers and
- * pinned staging are owned by an opaque context so repeated calls reuse them.
+ * ss_extrema, copies both masks back and synchronises.  Device buffers are
+ * owned by an opaque context, so repeated calls reuse them.
  * `elapsed_ms` (optional) receives the device time of the kernels alone;
  * `active_fragments` (optional) the fragment count. */
 typedef struct ss_context ss_context;
@@ -175,6 +192,15 @@ ss_status ss_extrema_batch(const void* h_plan, const void* d_plan,
                            size_t plan_bytes, int persistent,
                            void* d_workspace, size_t workspace_bytes,
                            void* stream);
+
+/* Split form of ss_extrema_batch: pass 1 is the tile pass, pass 2 the
+ * resolve pass.  Enqueuing pass 1 then pass 2 on one stream (other work may
+ * sit between them, e.g. timing events) is exactly ss_extrema_batch; the
+ * `persistent` flag must be the same for both passes. */
+ss_status ss_extrema_batch_pass(const void* h_plan, const void* d_plan,
+                                size_t plan_bytes, int persistent, int pass,
+                                void* d_workspace, size_t workspace_bytes,
+                                void* stream);
 
 #ifdef __cplusplus
 }

@@ -104,6 +104,9 @@ SIGNATURES = {
     "ss_batch_plan_fill": (_I, [ctypes.POINTER(ImageDesc), _I, _I, _VP, _SZ,
                                 ctypes.POINTER(_SZ)]),
     "ss_extrema_batch": (_I, [_VP, _VP, _SZ, _I, _VP, _SZ, _VP]),
+    "ss_extrema_batch_pass": (_I, [_VP, _VP, _SZ, _I, _I, _VP, _SZ, _VP]),
+    "ss_set_kernel_config": (_I, [_I, _I]),
+    "ss_get_kernel_config": (_I, [_I, ctypes.POINTER(_I)]),
 }
 
 
@@ -134,6 +137,21 @@ def _stream_handle(stream) -> int:
     if stream is None:
         stream = torch.cuda.current_stream()
     return int(stream.cuda_stream)
+
+
+def set_kernel_config(tile: int, warps: int) -> None:
+    """Selects the kernels used for `tile` (see ss_set_kernel_config)."""
+    _check(lib().ss_set_kernel_config(tile, warps), "ss_set_kernel_config")
+
+
+def get_kernel_config(tile: int) -> int:
+    out = ctypes.c_int(0)
+    _check(lib().ss_get_kernel_config(tile, ctypes.byref(out)),
+           "ss_get_kernel_config")
+    return int(out.value)
+
+
+KERNEL_CONFIGS = {16: (2, 4, 8), 32: (-4, -2, 4, 8, 16), 64: (8, 16)}
 
 
 def workspace_bytes(width: int, height: int, tile: int = 32) -> int:
@@ -279,6 +297,15 @@ class BatchPlan:
             self.plan_bytes, 1 if persistent else 0, workspace.ptr,
             workspace.nbytes, _stream_handle(stream))
         _check(st, "ss_extrema_batch")
+
+    def run_pass(self, workspace: Workspace, which: int,
+                 persistent: bool = False, stream=None) -> None:
+        """One pass of the split form: 1 = tile pass, 2 = resolve pass."""
+        st = lib().ss_extrema_batch_pass(
+            self.host_plan.ctypes.data, self.device_plan.data_ptr(),
+            self.plan_bytes, 1 if persistent else 0, which, workspace.ptr,
+            workspace.nbytes, _stream_handle(stream))
+        _check(st, "ss_extrema_batch_pass")
 
 
 def extrema_batch(images: Sequence, tile: int = 32, persistent: bool = False,

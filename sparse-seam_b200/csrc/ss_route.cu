@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "sparse_seam.h"
+#include "ss_rowscan.cuh"
 #include "ss_tile.cuh"
 
 namespace ss {
@@ -427,11 +428,93 @@ __global__ void init_header_kernel(Header* h) {
 }
 
 // ---------------------------------------------------------------------------
+// Row-scan kernels (T = 32): NW independent warps per CTA, one tile each.
+// ---------------------------------------------------------------------------
+
+template <int NW, bool kPersistent>
+__global__ void __launch_bounds__(NW * 32)
+rowscan_tile_pass_kernel(Source src, Arena a) {
+    __shared__ rowscan::WarpSmem sm[NW];
+    const int warp = static_cast<int>(threadIdx.x) >> 5;
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    if (a.header->magic != kMagic) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            raise_error(a.header, kErrUninitialized, 0u);
+        }
+        return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.header->last_tiles = static_cast<uint64_t>(src.total_tiles);
+        a.header->tile = rowscan::T;
+    }
+    if constexpr (kPersistent) {
+        for (;;) {
+            uint32_t item = 0;
+            if (lane == 0) {
+                item = atomicAdd(&a.header->queue_head, 1u);
+            }
+            item = __shfl_sync(~0u, item, 0);
+            if (static_cast<int64_t>(item) >= src.total_tiles) {
+                break;
+            }
+            rowscan::tile_pass_warp(sm[warp], src, a, item);
+            __syncwarp();
+        }
+    } else {
+        const int64_t item = static_cast<int64_t>(blockIdx.x) * NW + warp;
+        if (item < src.total_tiles) {
+            rowscan::tile_pass_warp(sm[warp], src, a, item);
+        }
+    }
+}
+
+template <int NW, bool kPersistent>
+__global__ void __launch_bounds__(NW * 32)
+rowscan_resolve_pass_kernel(Source src, Arena a) {
+    __shared__ rowscan::WarpSmem sm[NW];
+    const int warp = static_cast<int>(threadIdx.x) >> 5;
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    if (a.header->magic != kMagic) {
+        return;
+    }
+    if constexpr (kPersistent) {
+        for (;;) {
+            uint32_t item = 0;
+            if (lane == 0) {
+                item = atomicAdd(&a.header->resolve_head, 1u);
+            }
+            item = __shfl_sync(~0u, item, 0);
+            if (static_cast<int64_t>(item) >= src.total_tiles) {
+                break;
+            }
+            rowscan::resolve_warp(sm[warp], src, a, item);
+            __syncwarp();
+        }
+        // The last warp to finish rewinds both work queues for the next call.
+        if (lane == 0) {
+            __threadfence();
+            const uint32_t done = atomicAdd(&a.header->resolve_done, 1u);
+            if (done == gridDim.x * NW - 1) {
+                atomicExch(&a.header->queue_head, 0u);
+                atomicExch(&a.header->resolve_head, 0u);
+                atomicExch(&a.header->resolve_done, 0u);
+            }
+        }
+    } else {
+        const int64_t item = static_cast<int64_t>(blockIdx.x) * NW + warp;
+        if (item < src.total_tiles) {
+            rowscan::resolve_warp(sm[warp], src, a, item);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 
 struct Layout {
-    size_t relation, count, border, parent, bits, total;
+    size_t relation, count, border, parent, bits, pending_count, pending,
+        total;
 };
 
 static size_t round_up(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
@@ -467,6 +550,12 @@ static bool layout_for(int64_t tiles, int tile, size_t workspace_bytes,
     off = round_up(off + static_cast<size_t>(slots) * 4);
     L.bits = off;
     off = round_up(off + static_cast<size_t>(slots) * 4);
+    // The row-scan path (T = 32) logs pending runs: at most T * T per tile.
+    const size_t pend = tile == 32 ? static_cast<size_t>(tiles) : 0;
+    L.pending_count = off;
+    off = round_up(off + pend * 4);
+    L.pending = off;
+    off = round_up(off + pend * 32 * 32 * 4);
     L.total = off;
     *out = L;
     return L.total <= workspace_bytes &&
@@ -479,8 +568,10 @@ static bool workspace_size(int64_t tiles, int tile, size_t* bytes) {
         return false;
     }
     const size_t slots = static_cast<size_t>(tiles) * 4 * tile;
+    const size_t pend = tile == 32 ? static_cast<size_t>(tiles) : 0;
     const size_t dirty = round_up(static_cast<size_t>(tiles) * 2) +
-                         round_up(slots) + 2 * round_up(slots * 4);
+                         round_up(slots) + 2 * round_up(slots * 4) +
+                         round_up(pend * 4) + round_up(pend * 32 * 32 * 4);
     size_t s = round_up((dirty + 512) / 31 * 32 + 512);
     Layout L;
     for (int i = 0; i < 1024 && !layout_for(tiles, tile, s, &L); ++i) {
@@ -502,6 +593,8 @@ static Arena arena_at(void* base, const Layout& L) {
     a.border = reinterpret_cast<uint8_t*>(b + L.border);
     a.parent = reinterpret_cast<int32_t*>(b + L.parent);
     a.bits = reinterpret_cast<uint32_t*>(b + L.bits);
+    a.pending_count = reinterpret_cast<uint32_t*>(b + L.pending_count);
+    a.pending = reinterpret_cast<uint32_t*>(b + L.pending);
     return a;
 }
 
@@ -519,24 +612,37 @@ struct Config {
     int warps;
     Kernel tile_pass[2];
     Kernel resolve_pass[2];
+    int items_per_cta;   // tiles one CTA handles per launch slot
 };
 
 #define SS_CONFIG(T, NW)                                                      \
     Config {                                                                  \
         T, NW, {tile_pass_kernel<T, NW, false>, tile_pass_kernel<T, NW, true>}, \
             {resolve_pass_kernel<T, NW, false>,                               \
-             resolve_pass_kernel<T, NW, true>}                                \
+             resolve_pass_kernel<T, NW, true>}, 1                             \
+    }
+// Row-scan configurations are listed with warps = -NW (one tile per warp).
+#define SS_ROWSCAN(NW)                                                        \
+    Config {                                                                  \
+        32, -(NW),                                                            \
+            {rowscan_tile_pass_kernel<NW, false>,                             \
+             rowscan_tile_pass_kernel<NW, true>},                             \
+            {rowscan_resolve_pass_kernel<NW, false>,                          \
+             rowscan_resolve_pass_kernel<NW, true>}, NW                       \
     }
 
 static const Config kConfigs[] = {
     SS_CONFIG(16, 2), SS_CONFIG(16, 4), SS_CONFIG(16, 8),
     SS_CONFIG(32, 4), SS_CONFIG(32, 8), SS_CONFIG(32, 16),
     SS_CONFIG(64, 8), SS_CONFIG(64, 16),
+    SS_ROWSCAN(2), SS_ROWSCAN(4),
 };
 #undef SS_CONFIG
+#undef SS_ROWSCAN
 
-// Per tile size, the warps per CTA used by default (index by tile / 16 - 1).
-static std::atomic<int> g_default_warps[4] = {{4}, {8}, {0}, {16}};
+// Per tile size, the configuration used by default (index by tile / 16 - 1);
+// negative warps select the row-scan kernels.
+static std::atomic<int> g_default_warps[4] = {{4}, {-4}, {0}, {16}};
 
 static const Config* find_config(int tile, int warps) {
     for (const Config& c : kConfigs) {
@@ -582,11 +688,11 @@ static int persistent_grid(Kernel k, int threads) {
 
 static ss_status launch_route(const Config& cfg, const Source& src,
                               const Arena& arena, int persistent,
-                              cudaStream_t stream) {
+                              cudaStream_t stream, int passes = 3) {
     if (src.total_tiles == 0) {
         return SS_OK;
     }
-    const int threads = cfg.warps * 32;
+    const int threads = (cfg.warps < 0 ? -cfg.warps : cfg.warps) * 32;
     const int p = persistent ? 1 : 0;
     unsigned grid1;
     unsigned grid2;
@@ -596,13 +702,20 @@ static ss_status launch_route(const Config& cfg, const Source& src,
         if (g1 <= 0 || g2 <= 0) {
             return SS_ERR_CUDA;
         }
-        grid1 = static_cast<unsigned>(std::min<int64_t>(g1, src.total_tiles));
-        grid2 = static_cast<unsigned>(std::min<int64_t>(g2, src.total_tiles));
+        const int64_t ctas = (src.total_tiles + cfg.items_per_cta - 1) /
+                             cfg.items_per_cta;
+        grid1 = static_cast<unsigned>(std::min<int64_t>(g1, ctas));
+        grid2 = static_cast<unsigned>(std::min<int64_t>(g2, ctas));
     } else {
-        grid1 = grid2 = static_cast<unsigned>(src.total_tiles);
+        grid1 = grid2 = static_cast<unsigned>(
+            (src.total_tiles + cfg.items_per_cta - 1) / cfg.items_per_cta);
     }
-    cfg.tile_pass[p]<<<grid1, threads, 0, stream>>>(src, arena);
-    cfg.resolve_pass[p]<<<grid2, threads, 0, stream>>>(src, arena);
+    if (passes & 1) {
+        cfg.tile_pass[p]<<<grid1, threads, 0, stream>>>(src, arena);
+    }
+    if (passes & 2) {
+        cfg.resolve_pass[p]<<<grid2, threads, 0, stream>>>(src, arena);
+    }
     return cudaGetLastError() == cudaSuccess ? SS_OK : SS_ERR_CUDA;
 }
 
@@ -770,6 +883,28 @@ ss_status ss_read_status(void* d_workspace, size_t workspace_bytes,
     return h.error ? static_cast<ss_status>(h.error) : SS_OK;
 }
 
+ss_status ss_set_kernel_config(int tile, int warps) {
+    if (!tile_ok(tile)) {
+        return SS_ERR_UNSUPPORTED_TILE;
+    }
+    if (!find_config(tile, warps)) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    g_default_warps[tile / 16 - 1].store(warps);
+    return SS_OK;
+}
+
+ss_status ss_get_kernel_config(int tile, int* warps) {
+    if (!warps) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    if (!tile_ok(tile)) {
+        return SS_ERR_UNSUPPORTED_TILE;
+    }
+    *warps = g_default_warps[tile / 16 - 1].load();
+    return SS_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Batches
 // ---------------------------------------------------------------------------
@@ -861,10 +996,10 @@ ss_status ss_batch_plan_fill(const ss_image_desc* descs, int count, int tile,
     return SS_OK;
 }
 
-ss_status ss_extrema_batch(const void* h_plan, const void* d_plan,
-                           size_t plan_bytes, int persistent,
-                           void* d_workspace, size_t workspace_bytes,
-                           void* stream) {
+static ss_status batch_passes(const void* h_plan, const void* d_plan,
+                              size_t plan_bytes, int persistent,
+                              void* d_workspace, size_t workspace_bytes,
+                              void* stream, int passes) {
     if (!h_plan || !d_plan || !d_workspace ||
         plan_bytes < sizeof(PlanHeader)) {
         return SS_ERR_INVALID_VALUE;
@@ -904,7 +1039,26 @@ ss_status ss_extrema_batch(const void* h_plan, const void* d_plan,
     src.total_tiles = ph->total_tiles;
     return launch_route(*cfg, src, arena_at(d_workspace, L),
                         persistent ? 1 : 0,
-                        static_cast<cudaStream_t>(stream));
+                        static_cast<cudaStream_t>(stream), passes);
+}
+
+ss_status ss_extrema_batch(const void* h_plan, const void* d_plan,
+                           size_t plan_bytes, int persistent,
+                           void* d_workspace, size_t workspace_bytes,
+                           void* stream) {
+    return batch_passes(h_plan, d_plan, plan_bytes, persistent, d_workspace,
+                        workspace_bytes, stream, 3);
+}
+
+ss_status ss_extrema_batch_pass(const void* h_plan, const void* d_plan,
+                                size_t plan_bytes, int persistent, int pass,
+                                void* d_workspace, size_t workspace_bytes,
+                                void* stream) {
+    if (pass != 1 && pass != 2) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    return batch_passes(h_plan, d_plan, plan_bytes, persistent, d_workspace,
+                        workspace_bytes, stream, pass);
 }
 
 // ---------------------------------------------------------------------------

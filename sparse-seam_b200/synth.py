@@ -9,7 +9,11 @@ for them with the same sizes and value structure:
   smooth_noise        sum of three Gaussian-filtered white-noise fields
                       (sigma 1, 4, 16 px; weights 0.2, 0.3, 0.5), min-max
                       normalised to 0..255, plus uniform integer noise in
-                      [-2, 2], clamped -- natural-image-like
+                      [-2, 2], clamped -- natural-image-like.  Each filtered
+                      field is scaled to unit standard deviation before the
+                      weights apply; otherwise filtering alone would shrink
+                      the sigma-4 and sigma-16 fields to a few percent of the
+                      sigma-1 field and the sum would be close to white noise
   quantize            re-quantisation to L gray levels with the reference's
                       rule bin = (v*L) >> 8, out = round(bin*255/(L-1))
                       (harness/quantization_and_scaling/
@@ -85,8 +89,8 @@ def smooth_noise(height: int, width: int, seed: int = 0, device="cpu"):
         x = F.pad(noise, (r, r, 0, 0), mode="replicate")
         x = F.conv2d(x, taps.view(1, 1, 1, -1))
         x = F.pad(x, (0, 0, r, r), mode="replicate")
-        x = F.conv2d(x, taps.view(1, 1, -1, 1))
-        acc += weight * x[0, 0]
+        x = F.conv2d(x, taps.view(1, 1, -1, 1))[0, 0]
+        acc += weight * x / torch.clamp(x.std(), min=1e-12)
     lo, hi = acc.min(), acc.max()
     scaled = (acc - lo) * (255.0 / torch.clamp(hi - lo, min=1e-12))
     jitter = torch.randint(-2, 3, (height, width), generator=gen,

@@ -45,10 +45,13 @@ def test_workspace_bytes():
     b = pkg.workspace_bytes(1024, 1024, 32)
     c = pkg.workspace_bytes(1024, 1024, 64)
     assert a % 256 == 0 and b > a and c < b
-    # 2040x1356 at T=32: 64 x 43 tiles, 128 slots each, 9 bytes per slot
-    # plus border records and counters -> about 1.1 bytes per pixel.
+    # 2040x1356 at T=32: 64 x 43 tiles, 128 slots of 9 bytes each, border
+    # records, counters and a pending-run log of up to 32 x 32 entries of
+    # 4 bytes per tile -> about 5.4 bytes per pixel.
     w = pkg.workspace_bytes(2040, 1356, 32)
-    assert 2752 * 128 * 9 < w < 2040 * 1356 * 1.3
+    assert 2752 * (128 * 9 + 4096) < w < 2040 * 1356 * 5.6
+    # T=64 keeps no pending log: about 0.6 bytes per pixel.
+    assert pkg.workspace_bytes(2040, 1356, 64) < 2040 * 1356 * 0.7
     with pytest.raises(pkg.SparseSeamError) as e:
         pkg.workspace_bytes(100, 100, 48)
     assert e.value.status == 2
@@ -131,6 +134,23 @@ def test_batch_plan_is_built_on_the_host():
     # A bad descriptor is rejected.
     descs[2].pitch = 1
     assert lib.ss_batch_tiles(descs, len(sizes), 32, ctypes.byref(tiles)) == 1
+
+
+def test_kernel_config_hook():
+    pkg = package()
+    for tile, choices in pkg.KERNEL_CONFIGS.items():
+        default = pkg.get_kernel_config(tile)
+        assert default in choices
+        for w in choices:
+            pkg.set_kernel_config(tile, w)
+            assert pkg.get_kernel_config(tile) == w
+        pkg.set_kernel_config(tile, default)
+    with pytest.raises(pkg.SparseSeamError) as e:
+        pkg.set_kernel_config(32, 3)
+    assert e.value.status == 1
+    with pytest.raises(pkg.SparseSeamError) as e:
+        pkg.set_kernel_config(64, -4)
+    assert e.value.status == 1
 
 
 def test_missing_library_fails_loudly(tmp_path, monkeypatch):

@@ -74,10 +74,19 @@ def images():
     return out
 
 
-@pytest.mark.parametrize("tile", [32, 64])
-def test_product_matches_reference_routes(tile):
+@pytest.mark.parametrize("tile,warps", [(32, -4), (32, 8), (64, 16)])
+def test_product_matches_reference_routes(tile, warps):
     pkg = package()
     lib = ref_lib(tile)
+    before = pkg.get_kernel_config(tile)
+    pkg.set_kernel_config(tile, warps)
+    try:
+        check_against_reference(pkg, lib, tile, warps)
+    finally:
+        pkg.set_kernel_config(tile, before)
+
+
+def check_against_reference(pkg, lib, tile, warps):
     for img in images():
         h, w = img.shape
         d = torch.from_numpy(img).cuda()
@@ -89,5 +98,8 @@ def test_product_matches_reference_routes(tile):
         gmx, gmn, _ = reference_masks(lib, img, "globaluf")
         assert np.array_equal(got[0], smx) and np.array_equal(got[1], smn)
         assert np.array_equal(got[0], gmx) and np.array_equal(got[1], gmn)
-        assert stats.active_fragments == sfrag
         assert sfrag == int(oracle.tile_fragments(img, tile).sum())
+        if warps > 0:
+            assert stats.active_fragments == sfrag
+        else:
+            assert stats.active_fragments <= sfrag
