@@ -67,6 +67,10 @@ def parse_args():
                         "CPU baseline, reference GPU routes)")
     p.add_argument("--passes-only", action="store_true",
                    help="only run the split-pass loop (for profiling)")
+    p.add_argument("--levels", type=int, default=256,
+                   help="re-quantise the corpus to this many gray levels")
+    p.add_argument("--sweep", action="store_true",
+                   help="add the quantisation x tile sweep of the corpus")
     return p.parse_args()
 
 
@@ -194,11 +198,23 @@ def corpus_shapes(n_large: int, n_small: int):
     return [(1356, 2040)] * n_large + [(321, 481)] * n_small
 
 
-def make_corpus(n_large: int, n_small: int, seed_base: int, device):
+def make_corpus(n_large: int, n_small: int, seed_base: int, device,
+                levels: int = 256):
     from importlib import import_module
     synth = import_module("sparse-seam_b200.synth")
-    return [synth.smooth_noise(h, w, seed_base + i, device=device)
-            for i, (h, w) in enumerate(corpus_shapes(n_large, n_small))]
+    out = [synth.smooth_noise(h, w, seed_base + i, device=device)
+           for i, (h, w) in enumerate(corpus_shapes(n_large, n_small))]
+    if levels < 256:
+        out = [quantize_tensor(t, levels) for t in out]
+    return out
+
+
+def quantize_tensor(t, levels: int):
+    """The reference's re-quantisation rule on a device tensor
+    (harness/quantization_and_scaling/gpu_common_quant_v0_7.cu:479-494)."""
+    import torch
+    b = (t.to(torch.int32) * levels) >> 8
+    return ((b * 255 + (levels - 1) // 2) // (levels - 1)).to(torch.uint8)
 
 
 def peaks():
@@ -249,7 +265,7 @@ def run_reference_arm(args, dist: Dist):
         return 0
     device = "cuda" if torch.cuda.is_available() else "cpu"
     images = [t.cpu().numpy() for t in
-              make_corpus(args.large, args.small, 0, device)]
+              make_corpus(args.large, args.small, 0, device, args.levels)]
     threads = cpu_threads()
     pixels, _ = time_cpu_oracle(images, threads, reps=max(1, args.warmup))
     _, times = time_cpu_oracle(images, threads, reps=args.steps)
@@ -280,7 +296,8 @@ def run_reference_arm(args, dist: Dist):
 def config_dict(args):
     return {
         "workload": (f"natural-image-like corpus: {args.large} x 2040x1356 + "
-                     f"{args.small} x 481x321 uint8 smooth noise, 256 levels"),
+                     f"{args.small} x 481x321 uint8 smooth noise, "
+                     f"{args.levels} levels"),
         "tile": args.tile,
         "images_per_step": args.large + args.small,
         "pixels_per_step": sum(h * w for h, w in
@@ -364,7 +381,8 @@ def main():
     torch.cuda.set_device(device)
     tile = args.tile
 
-    images = make_corpus(args.large, args.small, 7919 * dist.rank, device)
+    images = make_corpus(args.large, args.small, 7919 * dist.rank, device,
+                         args.levels)
     pixels = sum(im.numel() for im in images)
     maxs = [torch.empty_like(im) for im in images]
     mins = [torch.empty_like(im) for im in images]
@@ -503,6 +521,8 @@ def main():
         "mismatches": mismatches,
     }
 
+    if args.sweep:
+        line["sweep"] = sweep(args, pkg, images, stream)
     if not args.quick:
         line.update(secondary(args, pkg, plan, images, host_images, maxs,
                               mins, stream, dist, hbm))
@@ -515,6 +535,49 @@ def main():
         print(json.dumps(line))
     dist.close()
     return 0
+
+
+def sweep(args, pkg, images, stream):
+    """Batched Gpix/s of the corpus re-quantised to 256/64/16/4/2 levels at
+    T = 16 / 32 / 64 (the reference's quantisation and tile-size studies),
+    each checked against the oracle on two images."""
+    import torch
+    import oracle
+    out = {}
+    pixels = sum(im.numel() for im in images)
+    for levels in (256, 64, 16, 4, 2):
+        imgs = images if levels == 256 else [quantize_tensor(t, levels)
+                                              for t in images]
+        maxs = [torch.empty_like(t) for t in imgs]
+        mins = [torch.empty_like(t) for t in imgs]
+        for tile in (16, 32, 64):
+            plan = pkg.BatchPlan(imgs, maxs, mins, tile=tile, stream=stream)
+            ws = plan.make_workspace(stream=stream)
+            best = None
+            for persistent in (False, True):
+                plan.run(ws, persistent=persistent, stream=stream)
+                stream.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(3):
+                    plan.run(ws, persistent=persistent, stream=stream)
+                e1.record(stream)
+                e1.synchronize()
+                ms = e0.elapsed_time(e1) / 3
+                best = ms if best is None else min(best, ms)
+            ws.read_status(stream)
+            bad = 0
+            for i in (0, len(imgs) - 1):
+                h = imgs[i].cpu().numpy()
+                wmx, wmn = oracle.extrema(h)
+                bad += int((maxs[i].cpu().numpy() != wmx).sum())
+                bad += int((mins[i].cpu().numpy() != wmn).sum())
+            out[f"q{levels}_t{tile}"] = {
+                "gpix_s": round(pixels / (best / 1e3) / 1e9, 3),
+                "ms": round(best, 4), "mismatches": bad}
+            del plan, ws
+    return out
 
 
 def secondary(args, pkg, plan, images, host_images, maxs, mins, stream, dist,

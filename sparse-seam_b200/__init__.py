@@ -179,9 +179,14 @@ class Workspace:
         return cls(workspace_bytes(width, height, tile), **kw)
 
     def init(self, stream=None) -> None:
+        """Resets the workspace and waits for the reset, so the workspace is
+        ready for work enqueued on any stream afterwards."""
+        import torch
+        st = stream or torch.cuda.current_stream(self.buffer.device)
         _check(lib().ss_workspace_init(self.ptr, self.nbytes,
-                                       _stream_handle(stream)),
+                                       _stream_handle(st)),
                "ss_workspace_init")
+        st.synchronize()
 
     def read_status(self, stream=None, raise_on_error: bool = True) -> Stats:
         stats = Stats()

@@ -471,7 +471,7 @@ rowscan_tile_pass_kernel(Source src, Arena a) {
 template <int NW, bool kPersistent>
 __global__ void __launch_bounds__(NW * 32)
 rowscan_resolve_pass_kernel(Source src, Arena a) {
-    __shared__ rowscan::WarpSmem sm[NW];
+    __shared__ rowscan::ResolveSmem sm[NW];
     const int warp = static_cast<int>(threadIdx.x) >> 5;
     const int lane = static_cast<int>(threadIdx.x) & 31;
     if (a.header->magic != kMagic) {

@@ -22,17 +22,17 @@
 //            harness/primary/snapshot_sparse_seam_cuda_v1_0.cu:213-281);
 //   phase D  flatten; each listed pixel ORs its flags into its root;
 //   phase E  in pixel order: live seam zones (touching a seam, flags not
-//            both set) get fragment records 0..k-1, the listed pixels'
-//            masks are written (provisional for live seam zones), and every
-//            pixel of a live seam zone is logged for the resolve pass;
+//            both set) get fragment records 0..k-1; listed pixels of the
+//            other zones get their masks; the pixels of live seam zones are
+//            logged as runs for the resolve pass;
 //   phase F  border records: the fragment record of each border pixel, or
 //            kDeadRecord when its zone is decided.
 //
 // Seam merging is wait-free: each pair of tiles joined by equal pixels owns a
 // counter and the second tile to arrive unites the pair's live fragments, or
 // ORs "both flags" into a live fragment whose partner across the seam is
-// dead.  The resolve pass compares every live fragment's own flags with its
-// component's and rewrites the logged pixels of the fragments that changed.
+// dead.  The resolve pass looks up every live fragment's component flags and
+// writes the logged runs, so every mask byte is written exactly once.
 #pragma once
 
 #include "ss_device.cuh"
@@ -47,6 +47,14 @@ constexpr int kPendingCap = T * T;     // logged pixels per tile
 constexpr uint8_t kDeadRecord = 0xFE;  // border record of a decided zone
 constexpr uint8_t kNoRecord = 0xFF;    // border pixel of a zone inside the tile
 
+// Run-log entry: bits 0-7 record, 8-13 x, 14-19 y, 20-26 length.
+__device__ __forceinline__ uint32_t pending_entry(int rec, int x, int y,
+                                                  int len) {
+    return static_cast<uint32_t>(rec) | (static_cast<uint32_t>(x) << 8) |
+           (static_cast<uint32_t>(y) << 14) |
+           (static_cast<uint32_t>(len) << 20);
+}
+
 // Per-pixel shared word: bits 0-9 parent, 10-12 zone flags (at roots),
 // 13-20 record + 1 (at roots of live seam zones), 21-23 own flags.
 constexpr uint32_t kParMask = 0x3FFu;
@@ -55,10 +63,13 @@ constexpr int kRecShift = 13;
 constexpr int kOwnShift = 21;
 constexpr uint32_t kDead = kHasGreater | kHasSmaller;
 
+constexpr int kHaloW = T + 2;   // staged tile rows: columns x0-1 .. x0+T
+
 struct __align__(16) WarpSmem {
     uint32_t word[T * T];
     uint16_t list[T * T];      // listed (undecided) pixels, in pixel order
     uint32_t listed[T];        // per row: listed pixels
+    int16_t img[kHaloW * kHaloW];  // tile + halo, -1 outside the image
     uint8_t final_flags[kSlots];
 };
 
@@ -98,15 +109,24 @@ __device__ __forceinline__ int pixel_at(const uint8_t* __restrict__ img,
                : -1;
 }
 
+// Find with path halving.  Used while linking (phase C), when a non-root
+// word changes only in its parent bits: halving rewrites those bits with an
+// ancestor, which is safe under concurrent linking and halving.
 __device__ __forceinline__ int wfind(volatile uint32_t* w, int x,
                                      uint32_t& err) {
 #pragma unroll 1
     for (int it = 0; it < T * T; ++it) {
-        const int p = static_cast<int>(w[x] & kParMask);
+        const uint32_t wx = w[x];
+        const int p = static_cast<int>(wx & kParMask);
         if (p == x) {
             return x;
         }
-        x = p;
+        const int gp = static_cast<int>(w[p] & kParMask);
+        if (gp == p) {
+            return p;
+        }
+        w[x] = (wx & ~kParMask) | static_cast<uint32_t>(gp);
+        x = gp;
     }
     err = kErrSpinLimit;
     return x;
@@ -158,38 +178,76 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
     uint8_t* __restrict__ omax = job.maxima;
     uint8_t* __restrict__ omin = job.minima;
 
+    // -- prologue: stage the tile and its halo --------------------------------
+    // Staged row r holds image row y0 - 1 + r, columns x0 - 1 .. x0 + T
+    // (staged column c = image column x0 - 1 + c); -1 outside the image.  All
+    // loads are issued before the first store so they overlap.
+    {
+        const int gx = g.x0 + lane;
+        const bool col_ok = lane < g.tw;
+        int vals[T + 2];
+#pragma unroll
+        for (int r = 0; r < T + 2; ++r) {
+            const int gy = g.y0 + r - 1;
+            vals[r] = (col_ok && static_cast<unsigned>(gy) <
+                                     static_cast<unsigned>(height))
+                          ? static_cast<int>(__ldg(img + gy * pitch + gx))
+                          : -1;
+        }
+        const int xl = g.x0 - 1;
+        const int xr = g.x0 + T;
+        const int gy0 = g.y0 - 1 + lane;
+        const int gy1 = g.y0 + 31 + lane;
+        const bool ok0 =
+            static_cast<unsigned>(gy0) < static_cast<unsigned>(height);
+        const bool ok1 = lane < 2 && static_cast<unsigned>(gy1) <
+                                         static_cast<unsigned>(height);
+        const int hl0 = (xl >= 0 && ok0)
+                            ? static_cast<int>(__ldg(img + gy0 * pitch + xl))
+                            : -1;
+        const int hr0 = (xr < width && ok0)
+                            ? static_cast<int>(__ldg(img + gy0 * pitch + xr))
+                            : -1;
+        const int hl1 = (xl >= 0 && ok1)
+                            ? static_cast<int>(__ldg(img + gy1 * pitch + xl))
+                            : -1;
+        const int hr1 = (xr < width && ok1)
+                            ? static_cast<int>(__ldg(img + gy1 * pitch + xr))
+                            : -1;
+#pragma unroll
+        for (int r = 0; r < T + 2; ++r) {
+            sm.img[r * kHaloW + lane + 1] = static_cast<int16_t>(vals[r]);
+        }
+        sm.img[lane * kHaloW] = static_cast<int16_t>(hl0);
+        sm.img[lane * kHaloW + kHaloW - 1] = static_cast<int16_t>(hr0);
+        if (lane < 2) {
+            sm.img[(32 + lane) * kHaloW] = static_cast<int16_t>(hl1);
+            sm.img[(32 + lane) * kHaloW + kHaloW - 1] =
+                static_cast<int16_t>(hr1);
+        }
+    }
+    __syncwarp();
+
     // -- phase A: flags, decided pixels, list ---------------------------------
     const bool col_ok = lane < g.tw;
-    const int gx = g.x0 + lane;
-    const bool halo_l = lane == 0 && g.x0 > 0;
-    const bool halo_r = lane == 31 && g.x0 + T < width;
-    auto load_row = [&](int y, int& v, int& L, int& R) {
-        const int gy = g.y0 + y;
-        const bool row_ok =
-            static_cast<unsigned>(gy) < static_cast<unsigned>(height);
-        const uint8_t* rowp = img + gy * pitch;
-        v = (row_ok && col_ok) ? static_cast<int>(__ldg(rowp + gx)) : -1;
-        int hl = -1;
-        int hr = -1;
-        if (row_ok && halo_l) hl = static_cast<int>(__ldg(rowp + g.x0 - 1));
-        if (row_ok && halo_r) hr = static_cast<int>(__ldg(rowp + g.x0 + T));
-        L = __shfl_up_sync(~0u, v, 1);
-        R = __shfl_down_sync(~0u, v, 1);
-        L = lane == 0 ? hl : L;
-        R = lane == 31 ? hr : R;
-    };
-    int vp, Lp, Rp, vc, Lc, Rc;
-    load_row(-1, vp, Lp, Rp);
-    load_row(0, vc, Lc, Rc);
-    int hmax_p = max(max(Lp, vp), Rp);
-    unsigned hmin_p =
-        min(min(static_cast<unsigned>(Lp), static_cast<unsigned>(vp)),
-            static_cast<unsigned>(Rp));
+    const int16_t* scol = sm.img + lane;   // staged column lane - 1 .. lane + 1
+    int Lc = scol[kHaloW];
+    int vc = scol[kHaloW + 1];
+    int Rc = scol[kHaloW + 2];
+    int hmax_p = max(max(static_cast<int>(scol[0]), static_cast<int>(scol[1])),
+                     static_cast<int>(scol[2]));
+    unsigned hmin_p = min(min(static_cast<unsigned>(scol[0]),
+                              static_cast<unsigned>(scol[1])),
+                          static_cast<unsigned>(scol[2]));
     int nlist = 0;
+    uint8_t* omax_row = omax + static_cast<int64_t>(g.y0) * out_pitch + g.x0 + lane;
+    uint8_t* omin_row = omin + static_cast<int64_t>(g.y0) * out_pitch + g.x0 + lane;
 #pragma unroll 2
     for (int y = 0; y < g.th; ++y) {
-        int vn, Ln, Rn;
-        load_row(y + 1, vn, Ln, Rn);
+        const int16_t* nrow = scol + (y + 2) * kHaloW;
+        const int Ln = nrow[0];
+        const int vn = nrow[1];
+        const int Rn = nrow[2];
         const int hmax_n = max(max(Ln, vn), Rn);
         const unsigned hmin_n =
             min(min(static_cast<unsigned>(Ln), static_cast<unsigned>(vn)),
@@ -201,10 +259,11 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
         const bool decided =
             col_ok && mx > vc && mn < static_cast<unsigned>(vc);
         if (decided) {
-            const int64_t o = (g.y0 + y) * out_pitch + gx;
-            omax[o] = 0;
-            omin[o] = 0;
+            *omax_row = 0;
+            *omin_row = 0;
         }
+        omax_row += out_pitch;
+        omin_row += out_pitch;
         const bool listed = col_ok && !decided;
         const uint32_t b = __ballot_sync(~0u, listed);
         if (listed) {
@@ -225,9 +284,6 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
     __syncwarp();
 
     // -- phase C: flags, seam, dead, links of listed pixels -------------------
-    // Interior tiles (all 8-neighbours inside the image) skip bounds checks.
-    const bool interior = g.x0 > 0 && g.y0 > 0 && g.x0 + T < width &&
-                          g.y0 + T < height;
     for (int base = 0; base < nlist; base += 32) {
         const int i = base + lane;
         const bool active = i < nlist;
@@ -238,27 +294,13 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
             p = sm.list[i];
             const int x = p & 31;
             const int y = p >> 5;
-            const int px = g.x0 + x;
-            const int py = g.y0 + y;
             int nb[9];
-            if (interior) {
-                const uint8_t* r0 = img + (py - 1) * pitch + px - 1;
+            const int16_t* w0 = sm.img + y * kHaloW + x;   // (x-1, y-1)
 #pragma unroll
-                for (int dy = 0; dy < 3; ++dy) {
+            for (int dy = 0; dy < 3; ++dy) {
 #pragma unroll
-                    for (int dx = 0; dx < 3; ++dx) {
-                        nb[dy * 3 + dx] =
-                            static_cast<int>(__ldg(r0 + dy * pitch + dx));
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int dy = 0; dy < 3; ++dy) {
-#pragma unroll
-                    for (int dx = 0; dx < 3; ++dx) {
-                        nb[dy * 3 + dx] = pixel_at(img, pitch, width, height,
-                                                   px + dx - 1, py + dy - 1);
-                    }
+                for (int dx = 0; dx < 3; ++dx) {
+                    nb[dy * 3 + dx] = w0[dy * kHaloW + dx];
                 }
             }
             const int v = nb[4];
@@ -353,9 +395,14 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
     }
     __syncwarp();
 
-    // -- phase E: records, masks of listed pixels, log ------------------------
+    // -- phase E: records, masks of listed pixels, run log --------------------
+    // Listed pixels of zones that are final here get their masks now.  Live
+    // seam zones are logged as runs (consecutive listed pixels of one row and
+    // one zone) and written once, by the resolve pass, with the component's
+    // flags.
     const int64_t frag_base = item * kSlots;
     uint32_t* plog = a.pending + item * kPendingCap;
+    const uint32_t le_mask = lt_mask | (1u << lane);
     int nrec = 0;
     int nlog = 0;
     for (int base = 0; base < nlist; base += 32) {
@@ -387,9 +434,9 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
         }
         nrec += __popc(fb);
         __syncwarp();
-        if (active) {
-            const int x = p & 31;
-            const int y = p >> 5;
+        const int x = p & 31;
+        const int y = p >> 5;
+        if (active && !live) {
             const int64_t o = (g.y0 + y) * out_pitch + g.x0 + x;
             omax[o] = (z & kHasGreater) ? 0 : 255;
             omin[o] = (z & kHasSmaller) ? 0 : 255;
@@ -398,13 +445,24 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
         if (live) {
             rec1 = (vw[root] >> kRecShift) & 0xFFu;
         }
-        const bool log = live && rec1 != 0u;
-        const uint32_t lb = __ballot_sync(~0u, log);
-        if (log) {
-            plog[nlog + __popc(lb & lt_mask)] =
-                static_cast<uint32_t>(p) | ((rec1 - 1u) << 10);
+        const bool logged = live && rec1 != 0u;
+        // Run continuation: the previous lane holds the left neighbour in
+        // the same zone (roots are equal exactly when zones are).
+        const int prev_p = __shfl_up_sync(~0u, p, 1);
+        const int prev_root = __shfl_up_sync(~0u, root, 1);
+        const bool prev_logged = __shfl_up_sync(~0u, logged, 1);
+        const bool cont = logged && lane > 0 && prev_logged &&
+                          prev_p == p - 1 && x != 0 && prev_root == root;
+        const bool head = logged && !cont;
+        const uint32_t stops = __ballot_sync(~0u, !cont);
+        const uint32_t hb = __ballot_sync(~0u, head);
+        if (head) {
+            const uint32_t later = stops & ~le_mask;
+            const int end = later ? __ffs(later) - 1 : 32;
+            plog[nlog + __popc(hb & lt_mask)] =
+                pending_entry(static_cast<int>(rec1 - 1u), x, y, end - lane);
         }
-        nlog += __popc(lb);
+        nlog += __popc(hb);
     }
     __syncwarp();
 
@@ -439,8 +497,9 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
     // -- seam relations --------------------------------------------------------
     // A relation is active when a pixel of this tile equals its 8-neighbour
     // across that seam; both tiles of the pair see the same pixel pairs.
-    auto own_px = [&](int x, int y) {
-        return pixel_at(img, pitch, width, height, g.x0 + x, g.y0 + y);
+    // Staged pixel (x, y) of the tile, x and y in -1 .. T (rows up to th).
+    auto own_px = [&](int x, int y) -> int {
+        return sm.img[(y + 1) * kHaloW + x + 1];
     };
     uint32_t rel = 0u;
     {
@@ -614,7 +673,12 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
 // Resolve pass (one warp, one tile)
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ void resolve_warp(WarpSmem& sm, const Source& src,
+struct __align__(16) ResolveSmem {
+    uint8_t final_flags[kSlots];
+};
+
+__device__ __forceinline__ void resolve_warp(ResolveSmem& sm,
+                                             const Source& src,
                                              const Arena& a, int64_t item) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
     // The tile pass is complete: clear this tile's seam-pair counters.
@@ -628,7 +692,7 @@ __device__ __forceinline__ void resolve_warp(WarpSmem& sm, const Source& src,
     uint32_t err = 0;
     const int count = a.fragment_count[item];
     const int64_t frag_base = item * kSlots;
-    uint32_t flips[kSlots / 32];
+    uint32_t any = 0u;
 #pragma unroll
     for (int i = 0; i < kSlots / 32; ++i) {
         const int r = lane + 32 * i;
@@ -641,46 +705,35 @@ __device__ __forceinline__ void resolve_warp(WarpSmem& sm, const Source& src,
             flip = comp != own;
             sm.final_flags[r] = static_cast<uint8_t>(comp);
         }
-        flips[i] = __ballot_sync(~0u, flip);
+        any |= __ballot_sync(~0u, flip);
     }
-    uint32_t any = 0u;
-#pragma unroll
-    for (int i = 0; i < kSlots / 32; ++i) {
-        any |= flips[i];
+    __syncwarp();
+    const PlanImage job = load_job(src, item);
+    const TileGeom g = tile_geom(job, item - job.tile_base);
+    const int64_t out_pitch = job.out_pitch;
+    const uint32_t* plog = a.pending + item * kPendingCap;
+    const uint32_t total = min(n, static_cast<uint32_t>(kPendingCap));
+    for (uint32_t e = lane; e < total; e += 32) {
+        const uint32_t ent = __ldcg(plog + e);
+        const int rec = static_cast<int>(ent & 0xFFu);
+        const int x = static_cast<int>((ent >> 8) & 63u);
+        const int y = static_cast<int>((ent >> 14) & 63u);
+        const int len = static_cast<int>((ent >> 20) & 127u);
+        if (rec >= count || x + len > g.tw || y >= g.th || len == 0) {
+            err = kErrRecordRange;
+            continue;
+        }
+        const uint32_t fl = sm.final_flags[rec];
+        const uint8_t mx = (fl & kHasGreater) ? 0 : 255;
+        const uint8_t mn = (fl & kHasSmaller) ? 0 : 255;
+        const int64_t o = (g.y0 + y) * out_pitch + g.x0 + x;
+        for (int k = 0; k < len; ++k) {
+            job.maxima[o + k] = mx;
+            job.minima[o + k] = mn;
+        }
     }
-    if (any) {
-        __syncwarp();
-        const PlanImage job = load_job(src, item);
-        const TileGeom g = tile_geom(job, item - job.tile_base);
-        const int64_t out_pitch = job.out_pitch;
-        const uint32_t* plog = a.pending + item * kPendingCap;
-        const uint32_t total = min(n, static_cast<uint32_t>(kPendingCap));
-        for (uint32_t e = lane; e < total; e += 32) {
-            const uint32_t ent = __ldcg(plog + e);
-            const int p = static_cast<int>(ent & 0x3FFu);
-            const int rec = static_cast<int>(ent >> 10);
-            const int x = p & 31;
-            const int y = p >> 5;
-            if (rec >= count || x >= g.tw || y >= g.th) {
-                err = kErrRecordRange;
-                continue;
-            }
-            uint32_t word = 0u;
-#pragma unroll
-            for (int i = 0; i < kSlots / 32; ++i) {
-                if ((rec >> 5) == i) word = flips[i];
-            }
-            if (!((word >> (rec & 31)) & 1u)) {
-                continue;
-            }
-            const uint32_t fl = sm.final_flags[rec];
-            const int64_t o = (g.y0 + y) * out_pitch + g.x0 + x;
-            job.maxima[o] = (fl & kHasGreater) ? 0 : 255;
-            job.minima[o] = (fl & kHasSmaller) ? 0 : 255;
-        }
-        if (lane == 0) {
-            atomicAdd(&a.header->flipped_tiles, 1u);
-        }
+    if (lane == 0 && any) {
+        atomicAdd(&a.header->flipped_tiles, 1u);
     }
     if (err) {
         raise_error(a.header, err, static_cast<uint32_t>(item));
