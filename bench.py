@@ -413,6 +413,7 @@ def main():
     if args.passes_only:
         for _ in range(max(1, args.steps)):
             plan.run_pass(ws, 1, stream=stream)
+            plan.run_pass(ws, 4, stream=stream)
             plan.run_pass(ws, 2, stream=stream)
         ws.read_status(stream)
         return 0
@@ -435,6 +436,8 @@ def main():
             lambda: plan.run(ws, persistent=persistent, stream=stream), 3)
     persistent = sched[True] < sched[False]
     ws.read_status(stream)
+
+    launches_per_run = 3 if pkg.get_kernel_config(tile) < 0 else 2
 
     # -- batched form, graph-replayed: the headline value ------------------
     graph = torch.cuda.CUDAGraph()
@@ -467,23 +470,21 @@ def main():
     stats = ws.read_status(stream)
 
     # -- per-pass timing (roofline of the tile pass) ----------------------
-    s1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    s2 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    t_pass1 = []
-    t_pass2 = []
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)]
+          for _ in range(args.steps)]
     for k in range(args.steps):
-        s1[k].record(stream)
+        ev[k][0].record(stream)
         plan.run_pass(ws, 1, persistent=persistent, stream=stream)
-        s2[k].record(stream)
+        ev[k][1].record(stream)
+        plan.run_pass(ws, 4, persistent=persistent, stream=stream)
+        ev[k][2].record(stream)
         plan.run_pass(ws, 2, persistent=persistent, stream=stream)
-        s1[k + 1].record(stream)
+        ev[k][3].record(stream)
     stream.synchronize()
-    for k in range(args.steps):
-        t_pass1.append(s1[k].elapsed_time(s2[k]))
-        t_pass2.append(s2[k].elapsed_time(s1[k + 1]))
+    tile_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
+    seam_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
+    resolve_ms = statistics.mean(e[2].elapsed_time(e[3]) for e in ev)
     ws.read_status(stream)
-    tile_ms = statistics.mean(t_pass1)
-    resolve_ms = statistics.mean(t_pass2)
     hbm, peak_kind = peaks()
     achieved = BYTES_PER_PIXEL * pixels / (tile_ms / 1e3) / 1e9
     traffic = committed_traffic()
@@ -501,8 +502,9 @@ def main():
         "schedule": {"persistent": persistent,
                      "ms_grid": round(sched[False], 4),
                      "ms_persistent": round(sched[True], 4)},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": launches_per_run * args.steps,
         "passes_ms": {"tile_pass": round(tile_ms, 4),
+                      "seam_pass": round(seam_ms, 4),
                       "resolve_pass": round(resolve_ms, 4)},
         "roofline": {"bound": "hbm", "kernel": "tile_pass_kernel",
                      "achieved": round(achieved, 2), "peak": hbm,
@@ -624,7 +626,7 @@ def secondary(args, pkg, plan, images, host_images, maxs, mins, stream, dist,
     out["per_image"] = {
         "value": round(pixels / (all_ms / 1e3) / 1e9, 4), "unit": UNIT,
         "ms_per_step": round(all_ms, 4),
-        "launches_per_image": 2,
+        "launches_per_image": 3 if pkg.get_kernel_config(tile) < 0 else 2,
     }
     if large_ms:
         px = 2040 * 1356

@@ -193,10 +193,11 @@ ss_status ss_extrema_batch(const void* h_plan, const void* d_plan,
                            void* d_workspace, size_t workspace_bytes,
                            void* stream);
 
-/* Split form of ss_extrema_batch: pass 1 is the tile pass, pass 2 the
- * resolve pass.  Enqueuing pass 1 then pass 2 on one stream (other work may
- * sit between them, e.g. timing events) is exactly ss_extrema_batch; the
- * `persistent` flag must be the same for both passes. */
+/* Split form of ss_extrema_batch: pass 1 is the tile pass, pass 4 the seam
+ * pass (row-scan kernels only; a no-op for the others), pass 2 the resolve
+ * pass.  Enqueuing passes 1, 4 and 2 in that order on one stream (other work
+ * may sit between them, e.g. timing events) is exactly ss_extrema_batch; the
+ * `persistent` flag must be the same for all passes. */
 ss_status ss_extrema_batch_pass(const void* h_plan, const void* d_plan,
                                 size_t plan_bytes, int persistent, int pass,
                                 void* d_workspace, size_t workspace_bytes,

@@ -305,7 +305,8 @@ class BatchPlan:
 
     def run_pass(self, workspace: Workspace, which: int,
                  persistent: bool = False, stream=None) -> None:
-        """One pass of the split form: 1 = tile pass, 2 = resolve pass."""
+        """One pass of the split form, enqueued in the order 1, 4, 2:
+        1 = tile pass, 4 = seam pass, 2 = resolve pass."""
         st = lib().ss_extrema_batch_pass(
             self.host_plan.ctypes.data, self.device_plan.data_ptr(),
             self.plan_bytes, 1 if persistent else 0, which, workspace.ptr,

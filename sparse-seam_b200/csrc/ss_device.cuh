@@ -115,8 +115,9 @@ struct Arena {
     int32_t* parent;         // [g * 4T + record]: fragment union-find
     uint32_t* bits;          // [g * 4T + record]: bits 0-1 zone flags (the
                              //   component's at a root), bits 8-9 own flags
-    uint32_t* pending_count; // [g]: pending-run entries (row-scan path)
-    uint32_t* pending;       // [g * T * T + e]: pending-run entries
+    uint32_t* pending_count; // [g]: run-log entries (row-scan path)
+    uint32_t* pending;       // [g * T * T + e]: run-log entries
+    uint32_t* seam_eq;       // [g * 8 + k]: seam equality words (row-scan)
 };
 
 // ---------------------------------------------------------------------------

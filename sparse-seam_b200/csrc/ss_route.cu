@@ -470,6 +470,20 @@ rowscan_tile_pass_kernel(Source src, Arena a) {
 
 template <int NW, bool kPersistent>
 __global__ void __launch_bounds__(NW * 32)
+rowscan_seam_pass_kernel(Source src, Arena a) {
+    (void)kPersistent;
+    if (a.header->magic != kMagic) {
+        return;
+    }
+    const int warp = static_cast<int>(threadIdx.x) >> 5;
+    const int64_t item = static_cast<int64_t>(blockIdx.x) * NW + warp;
+    if (item < src.total_tiles) {
+        rowscan::seam_pass_warp(src, a, item);
+    }
+}
+
+template <int NW, bool kPersistent>
+__global__ void __launch_bounds__(NW * 32)
 rowscan_resolve_pass_kernel(Source src, Arena a) {
     __shared__ rowscan::ResolveSmem sm[NW];
     const int warp = static_cast<int>(threadIdx.x) >> 5;
@@ -514,7 +528,7 @@ rowscan_resolve_pass_kernel(Source src, Arena a) {
 
 struct Layout {
     size_t relation, count, border, parent, bits, pending_count, pending,
-        total;
+        seam_eq, total;
 };
 
 static size_t round_up(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
@@ -556,6 +570,8 @@ static bool layout_for(int64_t tiles, int tile, size_t workspace_bytes,
     off = round_up(off + pend * 4);
     L.pending = off;
     off = round_up(off + pend * 32 * 32 * 4);
+    L.seam_eq = off;
+    off = round_up(off + pend * rowscan::kSeamWords * 4);
     L.total = off;
     *out = L;
     return L.total <= workspace_bytes &&
@@ -571,7 +587,8 @@ static bool workspace_size(int64_t tiles, int tile, size_t* bytes) {
     const size_t pend = tile == 32 ? static_cast<size_t>(tiles) : 0;
     const size_t dirty = round_up(static_cast<size_t>(tiles) * 2) +
                          round_up(slots) + 2 * round_up(slots * 4) +
-                         round_up(pend * 4) + round_up(pend * 32 * 32 * 4);
+                         round_up(pend * 4) + round_up(pend * 32 * 32 * 4) +
+                         round_up(pend * rowscan::kSeamWords * 4);
     size_t s = round_up((dirty + 512) / 31 * 32 + 512);
     Layout L;
     for (int i = 0; i < 1024 && !layout_for(tiles, tile, s, &L); ++i) {
@@ -595,6 +612,7 @@ static Arena arena_at(void* base, const Layout& L) {
     a.bits = reinterpret_cast<uint32_t*>(b + L.bits);
     a.pending_count = reinterpret_cast<uint32_t*>(b + L.pending_count);
     a.pending = reinterpret_cast<uint32_t*>(b + L.pending);
+    a.seam_eq = reinterpret_cast<uint32_t*>(b + L.seam_eq);
     return a;
 }
 
@@ -613,13 +631,14 @@ struct Config {
     Kernel tile_pass[2];
     Kernel resolve_pass[2];
     int items_per_cta;   // tiles one CTA handles per launch slot
+    Kernel seam_pass;    // between the two passes, or nullptr
 };
 
 #define SS_CONFIG(T, NW)                                                      \
     Config {                                                                  \
         T, NW, {tile_pass_kernel<T, NW, false>, tile_pass_kernel<T, NW, true>}, \
             {resolve_pass_kernel<T, NW, false>,                               \
-             resolve_pass_kernel<T, NW, true>}, 1                             \
+             resolve_pass_kernel<T, NW, true>}, 1, nullptr                    \
     }
 // Row-scan configurations are listed with warps = -NW (one tile per warp).
 #define SS_ROWSCAN(NW)                                                        \
@@ -628,7 +647,8 @@ struct Config {
             {rowscan_tile_pass_kernel<NW, false>,                             \
              rowscan_tile_pass_kernel<NW, true>},                             \
             {rowscan_resolve_pass_kernel<NW, false>,                          \
-             rowscan_resolve_pass_kernel<NW, true>}, NW                       \
+             rowscan_resolve_pass_kernel<NW, true>}, NW,                      \
+            rowscan_seam_pass_kernel<NW, false>                               \
     }
 
 static const Config kConfigs[] = {
@@ -688,7 +708,7 @@ static int persistent_grid(Kernel k, int threads) {
 
 static ss_status launch_route(const Config& cfg, const Source& src,
                               const Arena& arena, int persistent,
-                              cudaStream_t stream, int passes = 3) {
+                              cudaStream_t stream, int passes = 7) {
     if (src.total_tiles == 0) {
         return SS_OK;
     }
@@ -712,6 +732,11 @@ static ss_status launch_route(const Config& cfg, const Source& src,
     }
     if (passes & 1) {
         cfg.tile_pass[p]<<<grid1, threads, 0, stream>>>(src, arena);
+    }
+    if ((passes & 4) && cfg.seam_pass) {
+        const unsigned grid_seam = static_cast<unsigned>(
+            (src.total_tiles + cfg.items_per_cta - 1) / cfg.items_per_cta);
+        cfg.seam_pass<<<grid_seam, threads, 0, stream>>>(src, arena);
     }
     if (passes & 2) {
         cfg.resolve_pass[p]<<<grid2, threads, 0, stream>>>(src, arena);
@@ -1047,14 +1072,14 @@ ss_status ss_extrema_batch(const void* h_plan, const void* d_plan,
                            void* d_workspace, size_t workspace_bytes,
                            void* stream) {
     return batch_passes(h_plan, d_plan, plan_bytes, persistent, d_workspace,
-                        workspace_bytes, stream, 3);
+                        workspace_bytes, stream, 7);
 }
 
 ss_status ss_extrema_batch_pass(const void* h_plan, const void* d_plan,
                                 size_t plan_bytes, int persistent, int pass,
                                 void* d_workspace, size_t workspace_bytes,
                                 void* stream) {
-    if (pass != 1 && pass != 2) {
+    if (pass != 1 && pass != 2 && pass != 4) {
         return SS_ERR_INVALID_VALUE;
     }
     return batch_passes(h_plan, d_plan, plan_bytes, persistent, d_workspace,

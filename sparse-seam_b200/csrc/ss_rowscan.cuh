@@ -1,38 +1,46 @@
-// ss_rowscan.cuh -- warp-per-tile tile pass and list-driven resolve pass for
-// T = 32 (the reference's reported tile size).
+// ss_rowscan.cuh -- the T = 32 route (the reference's reported tile size):
+// a warp-per-tile tile pass, a seam pass and a list-driven resolve pass.
 //
 // Observation the design rests on: a pixel with both a strictly greater and a
 // strictly smaller 8-neighbour ("decided" pixel) is in neither mask, and
 // neither is any pixel of its flat zone (the zone's flags are the OR of its
 // pixels').  On natural images most pixels are decided, so only the others
-// need connectivity:
+// need connectivity.
 //
-//   phase A  row scan, lane = column, one warp instruction per 32 pixels:
-//            greater / smaller flags from sliding 3 x 3 row maxima / minima
-//            (outside pixels are -1, ignored by a signed max and an unsigned
-//            min); decided pixels get both masks 0 at once; the others are
-//            appended, in pixel order, to a per-warp list (ballot + popc);
-//   phase C  dense over the list: the 8 neighbours of each listed pixel give
-//            its flags, whether an equal neighbour lies outside the tile
-//            (seam), whether an equal neighbour inside the tile is decided
-//            (then the zone is decided too: "dead"), and its links: the first
-//            equal listed predecessor (up, up-left, up-right, left) becomes
-//            its parent and the left and up-right edges are united
-//            (Komura-style equivalence, as the reference's tile labelling,
-//            harness/primary/snapshot_sparse_seam_cuda_v1_0.cu:213-281);
-//   phase D  flatten; each listed pixel ORs its flags into its root;
-//   phase E  in pixel order: live seam zones (touching a seam, flags not
-//            both set) get fragment records 0..k-1; listed pixels of the
-//            other zones get their masks; the pixels of live seam zones are
-//            logged as runs for the resolve pass;
-//   phase F  border records: the fragment record of each border pixel, or
-//            kDeadRecord when its zone is decided.
+// Tile pass, one warp per 32 x 32 tile:
+//   prologue  the tile and its one-pixel halo are loaded (all loads in
+//             flight at once) and staged in shared memory as int16, -1
+//             outside the image;
+//   phase A   row scan, lane = column: greater / smaller flags from sliding
+//             3 x 3 row maxima / minima (a signed max and an unsigned min
+//             both ignore -1); decided pixels get both masks 0 at once; the
+//             others ("listed") are appended in pixel order to a per-warp
+//             list; per row, ballots record which pixels are listed and which
+//             continue a listed run of equal pixels from the left;
+//   phase C   dense over the list: flags, "seam" (an equal 8-neighbour outside
+//             the tile), "dead" (an equal decided neighbour inside the tile:
+//             the zone is decided too), and links.  A run member's parent is
+//             its run head; one union per pair of 8-adjacent equal runs in
+//             consecutive rows, issued at the first column of the pair's
+//             contact (three cases, see phase C);
+//   phase D   flatten; zone flags ORed into the roots, one atomic per root
+//             and warp step (lanes grouped by root with __match_any_sync);
+//   phase E   in pixel order: live seam zones (touching a seam, flags not
+//             both set) get fragment records 0..k-1 and are logged as runs;
+//             the other listed pixels get their masks;
+//   phase F   border records: each border pixel's fragment record, or
+//             kDeadRecord when its zone is decided; and the equalities across
+//             this tile's right and bottom seams, for the seam pass.
+// Seam pass, one warp per tile: every equal pair across the seams the tile
+//   owns (right, bottom, bottom-right, bottom-left) unites the two live
+//   fragments, or ORs "both flags" into a live fragment whose partner is dead.
+// Resolve pass, one warp per tile: looks up every live fragment's component
+//   flags and writes the logged runs; every mask byte is written once.
 //
-// Seam merging is wait-free: each pair of tiles joined by equal pixels owns a
-// counter and the second tile to arrive unites the pair's live fragments, or
-// ORs "both flags" into a live fragment whose partner across the seam is
-// dead.  The resolve pass looks up every live fragment's component flags and
-// writes the logged runs, so every mask byte is written exactly once.
+// Reference behaviour followed (paths inside the reference repository):
+// zone flags and seam test, harness/primary/snapshot_sparse_seam_cuda_v1_0.cu
+// :340-390; per-tile fragment records, :392-410; cross-seam merge of equal
+// 8-adjacent border pixels, :508-581; masks from the resolved flags, :477-506.
 #pragma once
 
 #include "ss_device.cuh"
@@ -43,17 +51,11 @@ namespace rowscan {
 
 constexpr int T = 32;
 constexpr int kSlots = 4 * T;          // fragment slots per tile
-constexpr int kPendingCap = T * T;     // logged pixels per tile
-constexpr uint8_t kDeadRecord = 0xFE;  // border record of a decided zone
-constexpr uint8_t kNoRecord = 0xFF;    // border pixel of a zone inside the tile
-
-// Run-log entry: bits 0-7 record, 8-13 x, 14-19 y, 20-26 length.
-__device__ __forceinline__ uint32_t pending_entry(int rec, int x, int y,
-                                                  int len) {
-    return static_cast<uint32_t>(rec) | (static_cast<uint32_t>(x) << 8) |
-           (static_cast<uint32_t>(y) << 14) |
-           (static_cast<uint32_t>(len) << 20);
-}
+constexpr int kPendingCap = T * T;     // run-log entries per tile
+constexpr int kHaloW = T + 2;          // staged row: columns x0-1 .. x0+T
+constexpr int kSeamWords = 8;          // seam equality words per tile
+constexpr uint32_t kDeadRecord = 0xFEu;  // border record of a decided zone
+constexpr uint32_t kNoRecord = 0xFFu;    // border pixel of an inside zone
 
 // Per-pixel shared word: bits 0-9 parent, 10-12 zone flags (at roots),
 // 13-20 record + 1 (at roots of live seam zones), 21-23 own flags.
@@ -63,13 +65,28 @@ constexpr int kRecShift = 13;
 constexpr int kOwnShift = 21;
 constexpr uint32_t kDead = kHasGreater | kHasSmaller;
 
-constexpr int kHaloW = T + 2;   // staged tile rows: columns x0-1 .. x0+T
+// Seam equality words of a tile: [0..2] right edge, bit y set when own pixel
+// (T-1, y) equals the right neighbour's (0, y + d), d = -1, 0, +1; [3..5]
+// bottom edge, bit x for own (x, T-1) and the lower neighbour's (x + d, 0);
+// [6] bit 0: bottom-right corner pair, bit 1: bottom-left corner pair.
+
+// Run-log entry: bits 0-7 record, 8-13 x, 14-19 y, 20-26 length.
+__device__ __forceinline__ uint32_t pending_entry(int rec, int x, int y,
+                                                  int len) {
+    return static_cast<uint32_t>(rec) | (static_cast<uint32_t>(x) << 8) |
+           (static_cast<uint32_t>(y) << 14) |
+           (static_cast<uint32_t>(len) << 20);
+}
 
 struct __align__(16) WarpSmem {
     uint32_t word[T * T];
-    uint16_t list[T * T];      // listed (undecided) pixels, in pixel order
-    uint32_t listed[T];        // per row: listed pixels
+    uint16_t list[T * T];          // listed pixels, in pixel order
+    uint32_t listed[T];            // per row: listed pixels
+    uint32_t cont[T];              // per row: listed run continuations
     int16_t img[kHaloW * kHaloW];  // tile + halo, -1 outside the image
+};
+
+struct __align__(16) ResolveSmem {
     uint8_t final_flags[kSlots];
 };
 
@@ -99,19 +116,14 @@ __device__ __forceinline__ PlanImage load_job(const Source& src,
     return src.images[idx];
 }
 
-// Pixel (gx, gy) of the image, or -1 outside it.
-__device__ __forceinline__ int pixel_at(const uint8_t* __restrict__ img,
-                                        int64_t pitch, int width, int height,
-                                        int gx, int gy) {
-    return (static_cast<unsigned>(gx) < static_cast<unsigned>(width) &&
-            static_cast<unsigned>(gy) < static_cast<unsigned>(height))
-               ? static_cast<int>(__ldg(img + gy * pitch + gx))
-               : -1;
+// Bits 0..x of a 32-bit row mask (x in 0..31).
+__device__ __forceinline__ uint32_t le_mask_of(int x) {
+    return (2u << x) - 1u;
 }
 
-// Find with path halving.  Used while linking (phase C), when a non-root
-// word changes only in its parent bits: halving rewrites those bits with an
-// ancestor, which is safe under concurrent linking and halving.
+// Find with path halving, used while linking (phase C): then a non-root
+// word changes only in its parent bits, and halving rewrites those bits with
+// an ancestor, which is safe under concurrent linking and halving.
 __device__ __forceinline__ int wfind(volatile uint32_t* w, int x,
                                      uint32_t& err) {
 #pragma unroll 1
@@ -132,8 +144,7 @@ __device__ __forceinline__ int wfind(volatile uint32_t* w, int x,
     return x;
 }
 
-// Links the larger root below the smaller one (CAS on the whole word; a
-// concurrent OR into the word's flag bits only makes the CAS retry).
+// Links the larger root below the smaller one (CAS on the whole word).
 __device__ __forceinline__ void wunion(uint32_t* w_, int a, int b,
                                        uint32_t& err) {
     volatile uint32_t* w = w_;
@@ -166,6 +177,7 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
                                                const Arena& a, int64_t item) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
     const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint32_t le_mask = lt_mask | (1u << lane);
     uint32_t err = 0;
 
     const PlanImage job = load_job(src, item);
@@ -179,9 +191,8 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
     uint8_t* __restrict__ omin = job.minima;
 
     // -- prologue: stage the tile and its halo --------------------------------
-    // Staged row r holds image row y0 - 1 + r, columns x0 - 1 .. x0 + T
-    // (staged column c = image column x0 - 1 + c); -1 outside the image.  All
-    // loads are issued before the first store so they overlap.
+    // Staged row r holds image row y0 - 1 + r, staged column c image column
+    // x0 - 1 + c.
     {
         const int gx = g.x0 + lane;
         const bool col_ok = lane < g.tw;
@@ -228,9 +239,9 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
     }
     __syncwarp();
 
-    // -- phase A: flags, decided pixels, list ---------------------------------
+    // -- phase A: flags, decided pixels, list, runs ----------------------------
     const bool col_ok = lane < g.tw;
-    const int16_t* scol = sm.img + lane;   // staged column lane - 1 .. lane + 1
+    const int16_t* scol = sm.img + lane;   // staged columns lane .. lane + 2
     int Lc = scol[kHaloW];
     int vc = scol[kHaloW + 1];
     int Rc = scol[kHaloW + 2];
@@ -240,8 +251,10 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
                               static_cast<unsigned>(scol[1])),
                           static_cast<unsigned>(scol[2]));
     int nlist = 0;
-    uint8_t* omax_row = omax + static_cast<int64_t>(g.y0) * out_pitch + g.x0 + lane;
-    uint8_t* omin_row = omin + static_cast<int64_t>(g.y0) * out_pitch + g.x0 + lane;
+    uint8_t* omax_row =
+        omax + static_cast<int64_t>(g.y0) * out_pitch + g.x0 + lane;
+    uint8_t* omin_row =
+        omin + static_cast<int64_t>(g.y0) * out_pitch + g.x0 + lane;
 #pragma unroll 2
     for (int y = 0; y < g.th; ++y) {
         const int16_t* nrow = scol + (y + 2) * kHaloW;
@@ -271,8 +284,12 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
                 static_cast<uint16_t>(y * T + lane);
         }
         nlist += __popc(b);
+        const bool cont = listed && lane > 0 && Lc == vc &&
+                          ((b >> (lane - 1)) & 1u);
+        const uint32_t cb = __ballot_sync(~0u, cont);
         if (lane == 0) {
             sm.listed[y] = b;
+            sm.cont[y] = cb;
         }
         hmax_p = max(max(Lc, vc), Rc);
         hmin_p = min(min(static_cast<unsigned>(Lc), static_cast<unsigned>(vc)),
@@ -284,12 +301,18 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
     __syncwarp();
 
     // -- phase C: flags, seam, dead, links of listed pixels -------------------
+    // Run R (value v) in row y is 8-adjacent to every listed run of row y-1
+    // with a pixel equal to v in columns [head - 1, end + 1]; those pixels form
+    // one segment per such run, and each segment's first column is hit by
+    // exactly one of: (a) a pixel x of R with eq-up and not eq-up-left, (b)
+    // the head of R with eq-up-left, (c) the end of R with eq-up-right and not
+    // eq-up ("eq" meaning equal and listed).
     for (int base = 0; base < nlist; base += 32) {
         const int i = base + lane;
         const bool active = i < nlist;
         int p = 0;
-        int link0 = -1;
-        int link1 = -1;
+        int t1 = -1;
+        int t2 = -1;
         if (active) {
             p = sm.list[i];
             const int x = p & 31;
@@ -304,56 +327,48 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
                 }
             }
             const int v = nb[4];
-            const uint32_t rows_up = y > 0 ? sm.listed[y - 1] : 0u;
-            const uint32_t rows_c = sm.listed[y];
-            const uint32_t rows_dn = y + 1 < g.th ? sm.listed[y + 1] : 0u;
+            const uint32_t up = y > 0 ? sm.listed[y - 1] : 0u;
+            const uint32_t cur = sm.listed[y];
+            const uint32_t dn = y + 1 < g.th ? sm.listed[y + 1] : 0u;
             bool gt = false, lt = false, seam = false, dead = false;
-            int parent = p;
-            bool have_parent = false;
-            // Visit order up, up-left, up-right, left, right, down-left,
-            // down, down-right (indices into the 3 x 3 window); the first
-            // equal listed predecessor becomes the parent.
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                // k -> window index: 0:U 1:UL 2:UR 3:L 4:R 5:DL 6:D 7:DR
-                const int n = k == 0 ? 1 : (k == 1 ? 0 : (k <= 3 ? k : k + 1));
+            for (int n = 0; n < 9; ++n) {
+                if (n == 4) continue;
                 const int dx = n % 3 - 1;
                 const int dy = n / 3 - 1;
                 const int nv = nb[n];
                 gt |= nv > v;
                 lt |= nv >= 0 && nv < v;
-                if (nv != v) {
-                    continue;
-                }
+                if (nv != v) continue;
                 const int qx = x + dx;
                 const int qy = y + dy;
                 if (qx < 0 || qx >= T || qy < 0 || qy >= T) {
                     seam = true;
                     continue;
                 }
-                const uint32_t rowmask =
-                    dy < 0 ? rows_up : (dy == 0 ? rows_c : rows_dn);
-                if (!((rowmask >> qx) & 1u)) {
+                const uint32_t row = dy < 0 ? up : (dy == 0 ? cur : dn);
+                if (!((row >> qx) & 1u)) {
                     dead = true;   // an equal decided pixel in the tile
-                    continue;
-                }
-                const bool backward = dy < 0 || (dy == 0 && dx < 0);
-                if (!backward) {
-                    continue;
-                }
-                const int q = qy * T + qx;
-                if (!have_parent) {
-                    parent = q;
-                    have_parent = true;
-                } else if (n == 2 || n == 3) {
-                    // up-right and left edges beyond the chosen parent
-                    if (link0 < 0) {
-                        link0 = q;
-                    } else {
-                        link1 = q;
-                    }
                 }
             }
+            const uint32_t cont_row = sm.cont[y];
+            const uint32_t heads = cur & ~cont_row;
+            const int head = 31 - __clz(heads & le_mask_of(x));
+            const bool eU = y > 0 && nb[1] == v && ((up >> x) & 1u);
+            const bool eUL = y > 0 && x > 0 && nb[0] == v &&
+                             ((up >> (x - 1)) & 1u);
+            const bool eUR = y > 0 && x < T - 1 && nb[2] == v &&
+                             ((up >> (x + 1)) & 1u);
+            const bool is_end = x == T - 1 || !((cont_row >> (x + 1)) & 1u);
+            if (eU && !eUL) {
+                t1 = p - T;
+            } else if (x == head && eUL) {
+                t1 = p - T - 1;
+            }
+            if (is_end && eUR && !eU) {
+                t2 = p - T + 1;
+            }
+            const int parent = x == head ? p : y * T + head;
             const uint32_t own = (gt ? kHasGreater : 0u) |
                                  (lt ? kHasSmaller : 0u) |
                                  (dead ? kDead : 0u) |
@@ -361,9 +376,9 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
             sm.word[p] = static_cast<uint32_t>(parent) | (own << kOwnShift);
         }
         __syncwarp();
-        if (__any_sync(~0u, link0 >= 0)) {
-            if (link0 >= 0) wunion(sm.word, p, link0, err);
-            if (link1 >= 0) wunion(sm.word, p, link1, err);
+        if (__any_sync(~0u, t1 >= 0 || t2 >= 0)) {
+            if (t1 >= 0) wunion(sm.word, p, t1, err);
+            if (t2 >= 0) wunion(sm.word, p, t2, err);
         }
         __syncwarp();
     }
@@ -372,37 +387,42 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
     volatile uint32_t* vw = sm.word;
     for (int base = 0; base < nlist; base += 32) {
         const int i = base + lane;
-        if (i < nlist) {
+        const bool active = i < nlist;
+        int root = -1 - lane;   // inactive lanes form groups of their own
+        uint32_t own = 0;
+        if (active) {
             const int p = sm.list[i];
-            int root = p;
+            root = p;
 #pragma unroll 1
             for (int it = 0; it < T * T; ++it) {
-                const int up = static_cast<int>(vw[root] & kParMask);
-                if (up == root) break;
-                root = up;
+                const int upp = static_cast<int>(vw[root] & kParMask);
+                if (upp == root) break;
+                root = upp;
             }
             const uint32_t wp = vw[p];
-            const uint32_t own = (wp >> kOwnShift) & 7u;
+            own = (wp >> kOwnShift) & 7u;
             if (root != p) {
                 // p is not a root: no other lane writes its word now.
                 vw[p] = (wp & ~kParMask) | static_cast<uint32_t>(root);
             }
+        }
+        const uint32_t group = __match_any_sync(~0u, root);
+        uint32_t agg = 0u;
+        agg |= (__ballot_sync(~0u, own & 1u) & group) ? 1u : 0u;
+        agg |= (__ballot_sync(~0u, own & 2u) & group) ? 2u : 0u;
+        agg |= (__ballot_sync(~0u, own & 4u) & group) ? 4u : 0u;
+        if (active && lane == __ffs(group) - 1) {
             const uint32_t zf = (vw[root] >> kZoneShift) & 7u;
-            if ((zf & own) != own) {
-                atomicOr(sm.word + root, own << kZoneShift);
+            if ((zf & agg) != agg) {
+                atomicOr(sm.word + root, agg << kZoneShift);
             }
         }
     }
     __syncwarp();
 
     // -- phase E: records, masks of listed pixels, run log --------------------
-    // Listed pixels of zones that are final here get their masks now.  Live
-    // seam zones are logged as runs (consecutive listed pixels of one row and
-    // one zone) and written once, by the resolve pass, with the component's
-    // flags.
     const int64_t frag_base = item * kSlots;
     uint32_t* plog = a.pending + item * kPendingCap;
-    const uint32_t le_mask = lt_mask | (1u << lane);
     int nrec = 0;
     int nlog = 0;
     for (int base = 0; base < nlist; base += 32) {
@@ -466,7 +486,7 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
     }
     __syncwarp();
 
-    // -- phase F: border records ----------------------------------------------
+    // -- phase F: border records, seam equalities ------------------------------
     uint8_t* border = a.border + item * kSlots;
     auto record_of = [&](int x, int y) -> uint32_t {
         if (!((sm.listed[y] >> x) & 1u)) {
@@ -489,180 +509,137 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
         border[2 * T + lane] = static_cast<uint8_t>(record_of(0, lane));
         border[3 * T + lane] = static_cast<uint8_t>(record_of(g.tw - 1, lane));
     }
+    // Staged pixel (x, y) of the tile, x and y in -1 .. T.
+    auto px = [&](int x, int y) -> int {
+        return sm.img[(y + 1) * kHaloW + x + 1];
+    };
+    const bool has_right = g.x0 + T < width;     // implies tw == T
+    const bool has_below = g.y0 + T < height;    // implies th == T
+    uint32_t eqw[kSeamWords];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const int y = lane;
+        const int y2 = y + d - 1;
+        const bool er = has_right && y < g.th && y2 >= 0 && y2 < g.th &&
+                        px(T - 1, y) == px(T, y2);
+        eqw[d] = __ballot_sync(~0u, er);
+        const int x = lane;
+        const int x2 = x + d - 1;
+        const bool eb = has_below && x < g.tw && x2 >= 0 && x2 < g.tw &&
+                        px(x, T - 1) == px(x2, T);
+        eqw[3 + d] = __ballot_sync(~0u, eb);
+    }
+    {
+        uint32_t corners = 0u;
+        if (has_right && has_below && px(T - 1, T - 1) == px(T, T)) {
+            corners |= 1u;
+        }
+        if (g.x0 > 0 && has_below && px(0, T - 1) == px(-1, T)) {
+            corners |= 2u;
+        }
+        eqw[6] = corners;
+        eqw[7] = 0u;
+    }
+    uint32_t mine = 0u;
+#pragma unroll
+    for (int k = 0; k < kSeamWords; ++k) {
+        if (lane == k) mine = eqw[k];
+    }
+    if (lane < kSeamWords) {
+        a.seam_eq[item * kSeamWords + lane] = mine;
+    }
     if (lane == 0) {
         a.fragment_count[item] = static_cast<uint16_t>(min(nrec, kSlots));
         a.pending_count[item] = static_cast<uint32_t>(nlog);
     }
+    if (err) {
+        raise_error(a.header, err, static_cast<uint32_t>(item));
+    }
+}
 
-    // -- seam relations --------------------------------------------------------
-    // A relation is active when a pixel of this tile equals its 8-neighbour
-    // across that seam; both tiles of the pair see the same pixel pairs.
-    // Staged pixel (x, y) of the tile, x and y in -1 .. T (rows up to th).
-    auto own_px = [&](int x, int y) -> int {
-        return sm.img[(y + 1) * kHaloW + x + 1];
-    };
-    uint32_t rel = 0u;
-    {
-        const int y = lane;   // left / right columns: lane = row
-        if (y < g.th) {
-            const int vl = own_px(0, y);
-            const int vr = own_px(g.tw - 1, y);
-            if (g.x0 > 0) {
-                for (int d = -1; d <= 1; ++d) {
-                    const int yy = y + d;
-                    if (own_px(-1, yy) == vl) {
-                        rel |= 1u << (yy < 0 ? kRelTopLeft
-                                             : (yy >= T ? kRelBottomLeft
-                                                        : kRelLeft));
-                    }
-                }
-            }
-            if (g.tw == T && g.x0 + T < width) {
-                for (int d = -1; d <= 1; ++d) {
-                    const int yy = y + d;
-                    if (own_px(T, yy) == vr) {
-                        rel |= 1u << (yy < 0 ? kRelTopRight
-                                             : (yy >= T ? kRelBottomRight
-                                                        : kRelRight));
-                    }
-                }
-            }
-        }
-        const int x = lane;   // top / bottom rows: lane = column
-        if (x < g.tw) {
-            const int vt = own_px(x, 0);
-            const int vb = own_px(x, g.th - 1);
-            if (g.y0 > 0) {
-                for (int d = -1; d <= 1; ++d) {
-                    const int xx = x + d;
-                    if (xx >= 0 && xx < T && own_px(xx, -1) == vt) {
-                        rel |= 1u << kRelTop;
-                    }
-                }
-            }
-            if (g.th == T && g.y0 + T < height) {
-                for (int d = -1; d <= 1; ++d) {
-                    const int xx = x + d;
-                    if (xx >= 0 && xx < T && own_px(xx, T) == vb) {
-                        rel |= 1u << kRelBottom;
-                    }
-                }
-            }
-        }
+// ---------------------------------------------------------------------------
+// Seam pass (one warp, the seams one tile owns)
+// ---------------------------------------------------------------------------
+
+// Joins the border pixel with record r1 of tile g1 to the equal pixel with
+// record r2 of tile g2.
+__device__ __forceinline__ void seam_join(const Arena& a, int64_t g1,
+                                          uint32_t r1, int64_t g2,
+                                          uint32_t r2, uint32_t& err) {
+    if (r1 == kNoRecord || r2 == kNoRecord) {
+        err = kErrInvariant;   // equal across a seam, yet no seam zone
+        return;
     }
-    rel = __reduce_or_sync(~0u, rel);
-    uint32_t second = 0u;
+    if ((r1 != kDeadRecord && r1 >= static_cast<uint32_t>(kSlots)) ||
+        (r2 != kDeadRecord && r2 >= static_cast<uint32_t>(kSlots))) {
+        err = kErrRecordRange;
+        return;
+    }
+    if (r1 == kDeadRecord && r2 == kDeadRecord) {
+        return;
+    }
+    const int f1 = static_cast<int>(g1 * kSlots + r1);
+    const int f2 = static_cast<int>(g2 * kSlots + r2);
+    if (r1 == kDeadRecord) {
+        global_or(a.parent, a.bits, f2, kDead, err);
+    } else if (r2 == kDeadRecord) {
+        global_or(a.parent, a.bits, f1, kDead, err);
+    } else {
+        global_union(a.parent, a.bits, f1, f2, err);
+    }
+}
+
+__device__ __forceinline__ void seam_pass_warp(const Source& src,
+                                               const Arena& a, int64_t item) {
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    const uint32_t* eq = a.seam_eq + item * kSeamWords;
+    const uint32_t mine = lane < kSeamWords ? __ldg(eq + lane) : 0u;
+    const uint32_t any = __reduce_or_sync(~0u, mine);
+    if (!any) {
+        return;
+    }
+    uint32_t eqw[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        eqw[k] = __shfl_sync(~0u, mine, k);
+    }
+    uint32_t err = 0;
+    const PlanImage job = load_job(src, item);
     const int64_t tiles_x = job.tiles_x;
-    if (rel) {
-        __threadfence();
-        __syncwarp();
-        uint32_t mine = 0u;
-        if (lane < 8 && ((rel >> lane) & 1u)) {
-            int64_t idx;
-            switch (lane) {
-                case kRelLeft: idx = (item - 1) * 4 + 0; break;
-                case kRelTop: idx = (item - tiles_x) * 4 + 1; break;
-                case kRelTopLeft: idx = (item - tiles_x - 1) * 4 + 2; break;
-                case kRelTopRight: idx = (item - tiles_x + 1) * 4 + 3; break;
-                case kRelRight: idx = item * 4 + 0; break;
-                case kRelBottom: idx = item * 4 + 1; break;
-                case kRelBottomRight: idx = item * 4 + 2; break;
-                default: idx = item * 4 + 3; break;
+    const uint8_t* own = a.border + item * kSlots;
+    if (eqw[0] | eqw[1] | eqw[2]) {
+        const int64_t ng = item + 1;
+        const uint8_t* nb = a.border + ng * kSlots;
+        const int y = lane;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if ((eqw[d] >> y) & 1u) {
+                seam_join(a, item, __ldg(own + 3 * T + y), ng,
+                          __ldg(nb + 2 * T + y + d - 1), err);
             }
-            const uint32_t old = atomicAdd(a.relation + idx, 1u);
-            if (old & 1u) {
-                mine = 1u << lane;
-            }
-        }
-        second = __reduce_or_sync(~0u, mine);
-        if (second) {
-            __threadfence();
         }
     }
-    // Joins own border pixel (ox, oy) with the outside pixel whose record is
-    // byte `off` of tile ng's border records.
-    auto join = [&](int ox, int oy, int64_t ng, int off) {
-        const uint32_t ro = record_of(ox, oy);
-        const uint32_t rn = ld_cg_u8(a.border + ng * kSlots + off);
-        const int64_t nbase = ng * kSlots;
-        if (ro == kNoRecord || rn == kNoRecord) {
-            err = kErrInvariant;   // equal across a seam, yet no seam zone
-            return;
-        }
-        if ((ro != kDeadRecord && ro >= static_cast<uint32_t>(kSlots)) ||
-            (rn != kDeadRecord && rn >= static_cast<uint32_t>(kSlots))) {
-            err = kErrRecordRange;
-            return;
-        }
-        if (ro == kDeadRecord && rn == kDeadRecord) {
-            return;
-        }
-        if (ro == kDeadRecord) {
-            global_or(a.parent, a.bits, static_cast<int>(nbase + rn), kDead,
-                      err);
-        } else if (rn == kDeadRecord) {
-            global_or(a.parent, a.bits, static_cast<int>(frag_base + ro),
-                      kDead, err);
-        } else {
-            global_union(a.parent, a.bits, static_cast<int>(frag_base + ro),
-                         static_cast<int>(nbase + rn), err);
-        }
-    };
-    while (second) {
-        const int r = __ffs(second) - 1;
-        second &= second - 1u;
-        if (r == kRelLeft || r == kRelRight) {
-            const bool left = r == kRelLeft;
-            const int64_t ng = left ? item - 1 : item + 1;
-            const int ox = left ? 0 : T - 1;
-            const int nx = left ? -1 : T;
-            const int side = left ? 3 : 2;   // neighbour's right / left column
-            const int y = lane;
-            if (y < g.th) {
-                const int v = own_px(ox, y);
-                for (int d = -1; d <= 1; ++d) {
-                    const int y2 = y + d;
-                    if (y2 < 0 || y2 >= g.th || own_px(nx, y2) != v) continue;
-                    join(ox, y, ng, side * T + y2);
-                }
-            }
-        } else if (r == kRelTop || r == kRelBottom) {
-            const bool top = r == kRelTop;
-            const int64_t ng = top ? item - tiles_x : item + tiles_x;
-            const int oy = top ? 0 : T - 1;
-            const int ny = top ? -1 : T;
-            const int side = top ? 1 : 0;    // neighbour's bottom / top row
-            const int x = lane;
-            if (x < g.tw) {
-                const int v = own_px(x, oy);
-                for (int d = -1; d <= 1; ++d) {
-                    const int x2 = x + d;
-                    if (x2 < 0 || x2 >= g.tw || own_px(x2, ny) != v) continue;
-                    join(x, oy, ng, side * T + x2);
-                }
-            }
-        } else if (lane == 0) {
-            int ox, oy, nx, ny, off;
-            int64_t ng;
-            switch (r) {
-                case kRelTopLeft:   // its bottom-right pixel
-                    ox = 0; oy = 0; nx = -1; ny = -1; off = T + (T - 1);
-                    ng = item - tiles_x - 1; break;
-                case kRelTopRight:  // its bottom-left pixel
-                    ox = T - 1; oy = 0; nx = T; ny = -1; off = T;
-                    ng = item - tiles_x + 1; break;
-                case kRelBottomRight:  // its top-left pixel
-                    ox = T - 1; oy = T - 1; nx = T; ny = T; off = 0;
-                    ng = item + tiles_x + 1; break;
-                default:  // bottom-left: its top-right pixel
-                    ox = 0; oy = T - 1; nx = -1; ny = T; off = T - 1;
-                    ng = item + tiles_x - 1; break;
-            }
-            const int v = own_px(ox, oy);
-            if (v >= 0 && own_px(nx, ny) == v) {
-                join(ox, oy, ng, off);
+    if (eqw[3] | eqw[4] | eqw[5]) {
+        const int64_t ng = item + tiles_x;
+        const uint8_t* nb = a.border + ng * kSlots;
+        const int x = lane;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if ((eqw[3 + d] >> x) & 1u) {
+                seam_join(a, item, __ldg(own + T + x), ng,
+                          __ldg(nb + x + d - 1), err);
             }
         }
+    }
+    if (lane == 0 && (eqw[6] & 1u)) {   // own (T-1, T-1), its (0, 0)
+        const int64_t ng = item + tiles_x + 1;
+        seam_join(a, item, __ldg(own + T + T - 1), ng,
+                  __ldg(a.border + ng * kSlots), err);
+    }
+    if (lane == 0 && (eqw[6] & 2u)) {   // own (0, T-1), its (T-1, 0)
+        const int64_t ng = item + tiles_x - 1;
+        seam_join(a, item, __ldg(own + T), ng,
+                  __ldg(a.border + ng * kSlots + T - 1), err);
     }
     if (err) {
         raise_error(a.header, err, static_cast<uint32_t>(item));
@@ -673,18 +650,10 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
 // Resolve pass (one warp, one tile)
 // ---------------------------------------------------------------------------
 
-struct __align__(16) ResolveSmem {
-    uint8_t final_flags[kSlots];
-};
-
 __device__ __forceinline__ void resolve_warp(ResolveSmem& sm,
                                              const Source& src,
                                              const Arena& a, int64_t item) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
-    // The tile pass is complete: clear this tile's seam-pair counters.
-    if (lane < 4) {
-        a.relation[item * 4 + lane] = 0u;
-    }
     const uint32_t n = a.pending_count[item];
     if (n == 0u) {
         return;
