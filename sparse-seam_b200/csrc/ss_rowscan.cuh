@@ -250,6 +250,9 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
     unsigned hmin_p = min(min(static_cast<unsigned>(scol[0]),
                               static_cast<unsigned>(scol[1])),
                           static_cast<unsigned>(scol[2]));
+    int hmax_c = max(max(Lc, vc), Rc);
+    unsigned hmin_c = min(min(static_cast<unsigned>(Lc), static_cast<unsigned>(vc)),
+                          static_cast<unsigned>(Rc));
     int nlist = 0;
     uint8_t* omax_row =
         omax + static_cast<int64_t>(g.y0) * out_pitch + g.x0 + lane;
@@ -269,8 +272,9 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
         const unsigned mn = min(min(hmin_p, hmin_n),
                                 min(static_cast<unsigned>(Lc),
                                     static_cast<unsigned>(Rc)));
-        const bool decided =
-            col_ok && mx > vc && mn < static_cast<unsigned>(vc);
+        const bool gt = mx > vc;
+        const bool lt = mn < static_cast<unsigned>(vc);
+        const bool decided = col_ok && gt && lt;
         if (decided) {
             *omax_row = 0;
             *omin_row = 0;
@@ -280,8 +284,9 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
         const bool listed = col_ok && !decided;
         const uint32_t b = __ballot_sync(~0u, listed);
         if (listed) {
-            sm.list[nlist + __popc(b & lt_mask)] =
-                static_cast<uint16_t>(y * T + lane);
+            // Entry: pixel index, then its greater / smaller flags.
+            sm.list[nlist + __popc(b & lt_mask)] = static_cast<uint16_t>(
+                (y * T + lane) | (gt ? 1u << 10 : 0u) | (lt ? 1u << 11 : 0u));
         }
         nlist += __popc(b);
         const bool cont = listed && lane > 0 && Lc == vc &&
@@ -291,9 +296,10 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
             sm.listed[y] = b;
             sm.cont[y] = cb;
         }
-        hmax_p = max(max(Lc, vc), Rc);
-        hmin_p = min(min(static_cast<unsigned>(Lc), static_cast<unsigned>(vc)),
-                     static_cast<unsigned>(Rc));
+        hmax_p = hmax_c;
+        hmin_p = hmin_c;
+        hmax_c = hmax_n;
+        hmin_c = hmin_n;
         vc = vn;
         Lc = Ln;
         Rc = Rn;
@@ -307,6 +313,9 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
     // exactly one of: (a) a pixel x of R with eq-up and not eq-up-left, (b)
     // the head of R with eq-up-left, (c) the end of R with eq-up-right and not
     // eq-up ("eq" meaning equal and listed).
+    // The 3 x 3 window is handled as bit sets, bit n = 3 * (dy + 1) + (dx + 1)
+    // (centre bit 4 unused): which neighbours are equal, which lie outside
+    // the tile, which are listed.
     for (int base = 0; base < nlist; base += 32) {
         const int i = base + lane;
         const bool active = i < nlist;
@@ -314,51 +323,44 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
         int t1 = -1;
         int t2 = -1;
         if (active) {
-            p = sm.list[i];
+            const uint32_t ent = sm.list[i];
+            p = static_cast<int>(ent & 1023u);
             const int x = p & 31;
             const int y = p >> 5;
-            int nb[9];
             const int16_t* w0 = sm.img + y * kHaloW + x;   // (x-1, y-1)
+            const int v = w0[kHaloW + 1];
+            uint32_t eq = 0u;
 #pragma unroll
             for (int dy = 0; dy < 3; ++dy) {
 #pragma unroll
                 for (int dx = 0; dx < 3; ++dx) {
-                    nb[dy * 3 + dx] = w0[dy * kHaloW + dx];
+                    if (dy == 1 && dx == 1) continue;
+                    eq |= (static_cast<int>(w0[dy * kHaloW + dx]) == v)
+                              ? 1u << (dy * 3 + dx) : 0u;
                 }
             }
-            const int v = nb[4];
-            const uint32_t up = y > 0 ? sm.listed[y - 1] : 0u;
-            const uint32_t cur = sm.listed[y];
-            const uint32_t dn = y + 1 < g.th ? sm.listed[y + 1] : 0u;
-            bool gt = false, lt = false, seam = false, dead = false;
-#pragma unroll
-            for (int n = 0; n < 9; ++n) {
-                if (n == 4) continue;
-                const int dx = n % 3 - 1;
-                const int dy = n / 3 - 1;
-                const int nv = nb[n];
-                gt |= nv > v;
-                lt |= nv >= 0 && nv < v;
-                if (nv != v) continue;
-                const int qx = x + dx;
-                const int qy = y + dy;
-                if (qx < 0 || qx >= T || qy < 0 || qy >= T) {
-                    seam = true;
-                    continue;
-                }
-                const uint32_t row = dy < 0 ? up : (dy == 0 ? cur : dn);
-                if (!((row >> qx) & 1u)) {
-                    dead = true;   // an equal decided pixel in the tile
-                }
-            }
+            const uint64_t up = y > 0 ? sm.listed[y - 1] : 0u;
+            const uint64_t cur = sm.listed[y];
+            const uint64_t dn = y + 1 < g.th ? sm.listed[y + 1] : 0u;
+            // Column x - 1 .. x + 1 of a row mask as 3 bits (column -1 and
+            // column 32 read as unlisted).
+            const uint32_t lw =
+                static_cast<uint32_t>(((up << 1) >> x) & 7u) |
+                (static_cast<uint32_t>(((cur << 1) >> x) & 7u) << 3) |
+                (static_cast<uint32_t>(((dn << 1) >> x) & 7u) << 6);
+            const uint32_t outside = (x == 0 ? 0x049u : 0u) |
+                                     (x == T - 1 ? 0x124u : 0u) |
+                                     (y == 0 ? 0x007u : 0u) |
+                                     (y == T - 1 ? 0x1C0u : 0u);
+            const bool seam = (eq & outside) != 0u;
+            const bool dead = (eq & ~outside & ~lw) != 0u;
+            const uint32_t eql = eq & lw & ~outside;   // equal and listed
+            const bool eUL = eql & 1u;
+            const bool eU = (eql >> 1) & 1u;
+            const bool eUR = (eql >> 2) & 1u;
             const uint32_t cont_row = sm.cont[y];
-            const uint32_t heads = cur & ~cont_row;
+            const uint32_t heads = static_cast<uint32_t>(cur) & ~cont_row;
             const int head = 31 - __clz(heads & le_mask_of(x));
-            const bool eU = y > 0 && nb[1] == v && ((up >> x) & 1u);
-            const bool eUL = y > 0 && x > 0 && nb[0] == v &&
-                             ((up >> (x - 1)) & 1u);
-            const bool eUR = y > 0 && x < T - 1 && nb[2] == v &&
-                             ((up >> (x + 1)) & 1u);
             const bool is_end = x == T - 1 || !((cont_row >> (x + 1)) & 1u);
             if (eU && !eUL) {
                 t1 = p - T;
@@ -369,9 +371,7 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
                 t2 = p - T + 1;
             }
             const int parent = x == head ? p : y * T + head;
-            const uint32_t own = (gt ? kHasGreater : 0u) |
-                                 (lt ? kHasSmaller : 0u) |
-                                 (dead ? kDead : 0u) |
+            const uint32_t own = ((ent >> 10) & 3u) | (dead ? kDead : 0u) |
                                  (seam ? kTouchesSeam : 0u);
             sm.word[p] = static_cast<uint32_t>(parent) | (own << kOwnShift);
         }
@@ -391,7 +391,7 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
         int root = -1 - lane;   // inactive lanes form groups of their own
         uint32_t own = 0;
         if (active) {
-            const int p = sm.list[i];
+            const int p = sm.list[i] & 1023;
             root = p;
 #pragma unroll 1
             for (int it = 0; it < T * T; ++it) {
@@ -432,7 +432,7 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
         int root = 0;
         uint32_t z = 0;
         if (active) {
-            p = sm.list[i];
+            p = sm.list[i] & 1023;
             root = static_cast<int>(vw[p] & kParMask);
             z = (vw[root] >> kZoneShift) & 7u;
         }
