@@ -117,7 +117,8 @@ struct Arena {
                              //   component's at a root), bits 8-9 own flags
     uint32_t* pending_count; // [g]: run-log entries (row-scan path)
     uint32_t* pending;       // [g * T * T + e]: run-log entries
-    uint32_t* seam_eq;       // [g * 8 + k]: seam equality words (row-scan)
+    uint32_t* seam_count;    // [g]: seam items (row-scan path)
+    uint32_t* seam_items;    // [g * 12T + i]: seam items (row-scan path)
 };
 
 // ---------------------------------------------------------------------------

@@ -468,6 +468,7 @@ rowscan_tile_pass_kernel(Source src, Arena a) {
     }
 }
 
+// Seam and resolve passes: each warp takes 32 consecutive tiles.
 template <int NW, bool kPersistent>
 __global__ void __launch_bounds__(NW * 32)
 rowscan_seam_pass_kernel(Source src, Arena a) {
@@ -476,9 +477,10 @@ rowscan_seam_pass_kernel(Source src, Arena a) {
         return;
     }
     const int warp = static_cast<int>(threadIdx.x) >> 5;
-    const int64_t item = static_cast<int64_t>(blockIdx.x) * NW + warp;
-    if (item < src.total_tiles) {
-        rowscan::seam_pass_warp(src, a, item);
+    const int64_t first =
+        (static_cast<int64_t>(blockIdx.x) * NW + warp) * 32;
+    if (first < src.total_tiles) {
+        rowscan::seam_pass_warp32(src, a, first);
     }
 }
 
@@ -493,15 +495,16 @@ rowscan_resolve_pass_kernel(Source src, Arena a) {
     }
     if constexpr (kPersistent) {
         for (;;) {
-            uint32_t item = 0;
+            uint32_t group = 0;
             if (lane == 0) {
-                item = atomicAdd(&a.header->resolve_head, 1u);
+                group = atomicAdd(&a.header->resolve_head, 1u);
             }
-            item = __shfl_sync(~0u, item, 0);
-            if (static_cast<int64_t>(item) >= src.total_tiles) {
+            group = __shfl_sync(~0u, group, 0);
+            const int64_t first = static_cast<int64_t>(group) * 32;
+            if (first >= src.total_tiles) {
                 break;
             }
-            rowscan::resolve_warp(sm[warp], src, a, item);
+            rowscan::resolve_warp32(sm[warp], src, a, first);
             __syncwarp();
         }
         // The last warp to finish rewinds both work queues for the next call.
@@ -515,9 +518,10 @@ rowscan_resolve_pass_kernel(Source src, Arena a) {
             }
         }
     } else {
-        const int64_t item = static_cast<int64_t>(blockIdx.x) * NW + warp;
-        if (item < src.total_tiles) {
-            rowscan::resolve_warp(sm[warp], src, a, item);
+        const int64_t first =
+            (static_cast<int64_t>(blockIdx.x) * NW + warp) * 32;
+        if (first < src.total_tiles) {
+            rowscan::resolve_warp32(sm[warp], src, a, first);
         }
     }
 }
@@ -528,7 +532,7 @@ rowscan_resolve_pass_kernel(Source src, Arena a) {
 
 struct Layout {
     size_t relation, count, border, parent, bits, pending_count, pending,
-        seam_eq, total;
+        seam_count, seam_items, total;
 };
 
 static size_t round_up(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
@@ -570,8 +574,10 @@ static bool layout_for(int64_t tiles, int tile, size_t workspace_bytes,
     off = round_up(off + pend * 4);
     L.pending = off;
     off = round_up(off + pend * 32 * 32 * 4);
-    L.seam_eq = off;
-    off = round_up(off + pend * rowscan::kSeamWords * 4);
+    L.seam_count = off;
+    off = round_up(off + pend * 4);
+    L.seam_items = off;
+    off = round_up(off + pend * rowscan::kSeamCap * 4);
     L.total = off;
     *out = L;
     return L.total <= workspace_bytes &&
@@ -588,7 +594,8 @@ static bool workspace_size(int64_t tiles, int tile, size_t* bytes) {
     const size_t dirty = round_up(static_cast<size_t>(tiles) * 2) +
                          round_up(slots) + 2 * round_up(slots * 4) +
                          round_up(pend * 4) + round_up(pend * 32 * 32 * 4) +
-                         round_up(pend * rowscan::kSeamWords * 4);
+                         round_up(pend * 4) +
+                         round_up(pend * rowscan::kSeamCap * 4);
     size_t s = round_up((dirty + 512) / 31 * 32 + 512);
     Layout L;
     for (int i = 0; i < 1024 && !layout_for(tiles, tile, s, &L); ++i) {
@@ -612,7 +619,8 @@ static Arena arena_at(void* base, const Layout& L) {
     a.bits = reinterpret_cast<uint32_t*>(b + L.bits);
     a.pending_count = reinterpret_cast<uint32_t*>(b + L.pending_count);
     a.pending = reinterpret_cast<uint32_t*>(b + L.pending);
-    a.seam_eq = reinterpret_cast<uint32_t*>(b + L.seam_eq);
+    a.seam_count = reinterpret_cast<uint32_t*>(b + L.seam_count);
+    a.seam_items = reinterpret_cast<uint32_t*>(b + L.seam_items);
     return a;
 }
 
@@ -630,15 +638,16 @@ struct Config {
     int warps;
     Kernel tile_pass[2];
     Kernel resolve_pass[2];
-    int items_per_cta;   // tiles one CTA handles per launch slot
+    int items_per_cta;   // tiles one tile-pass CTA handles per launch slot
     Kernel seam_pass;    // between the two passes, or nullptr
+    int later_per_cta;   // tiles one seam / resolve CTA handles
 };
 
 #define SS_CONFIG(T, NW)                                                      \
     Config {                                                                  \
         T, NW, {tile_pass_kernel<T, NW, false>, tile_pass_kernel<T, NW, true>}, \
             {resolve_pass_kernel<T, NW, false>,                               \
-             resolve_pass_kernel<T, NW, true>}, 1, nullptr                    \
+             resolve_pass_kernel<T, NW, true>}, 1, nullptr, 1                 \
     }
 // Row-scan configurations are listed with warps = -NW (one tile per warp).
 #define SS_ROWSCAN(NW)                                                        \
@@ -648,7 +657,7 @@ struct Config {
              rowscan_tile_pass_kernel<NW, true>},                             \
             {rowscan_resolve_pass_kernel<NW, false>,                          \
              rowscan_resolve_pass_kernel<NW, true>}, NW,                      \
-            rowscan_seam_pass_kernel<NW, false>                               \
+            rowscan_seam_pass_kernel<NW, false>, 32 * NW                      \
     }
 
 static const Config kConfigs[] = {
@@ -722,20 +731,24 @@ static ss_status launch_route(const Config& cfg, const Source& src,
         if (g1 <= 0 || g2 <= 0) {
             return SS_ERR_CUDA;
         }
-        const int64_t ctas = (src.total_tiles + cfg.items_per_cta - 1) /
-                             cfg.items_per_cta;
-        grid1 = static_cast<unsigned>(std::min<int64_t>(g1, ctas));
-        grid2 = static_cast<unsigned>(std::min<int64_t>(g2, ctas));
+        const int64_t ctas1 = (src.total_tiles + cfg.items_per_cta - 1) /
+                              cfg.items_per_cta;
+        const int64_t ctas2 = (src.total_tiles + cfg.later_per_cta - 1) /
+                              cfg.later_per_cta;
+        grid1 = static_cast<unsigned>(std::min<int64_t>(g1, ctas1));
+        grid2 = static_cast<unsigned>(std::min<int64_t>(g2, ctas2));
     } else {
-        grid1 = grid2 = static_cast<unsigned>(
+        grid1 = static_cast<unsigned>(
             (src.total_tiles + cfg.items_per_cta - 1) / cfg.items_per_cta);
+        grid2 = static_cast<unsigned>(
+            (src.total_tiles + cfg.later_per_cta - 1) / cfg.later_per_cta);
     }
     if (passes & 1) {
         cfg.tile_pass[p]<<<grid1, threads, 0, stream>>>(src, arena);
     }
     if ((passes & 4) && cfg.seam_pass) {
         const unsigned grid_seam = static_cast<unsigned>(
-            (src.total_tiles + cfg.items_per_cta - 1) / cfg.items_per_cta);
+            (src.total_tiles + cfg.later_per_cta - 1) / cfg.later_per_cta);
         cfg.seam_pass<<<grid_seam, threads, 0, stream>>>(src, arena);
     }
     if (passes & 2) {

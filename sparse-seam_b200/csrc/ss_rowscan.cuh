@@ -53,7 +53,7 @@ constexpr int T = 32;
 constexpr int kSlots = 4 * T;          // fragment slots per tile
 constexpr int kPendingCap = T * T;     // run-log entries per tile
 constexpr int kHaloW = T + 2;          // staged row: columns x0-1 .. x0+T
-constexpr int kSeamWords = 8;          // seam equality words per tile
+constexpr int kSeamCap = 12 * T;       // seam items per tile
 constexpr uint32_t kDeadRecord = 0xFEu;  // border record of a decided zone
 constexpr uint32_t kNoRecord = 0xFFu;    // border pixel of an inside zone
 
@@ -65,10 +65,8 @@ constexpr int kRecShift = 13;
 constexpr int kOwnShift = 21;
 constexpr uint32_t kDead = kHasGreater | kHasSmaller;
 
-// Seam equality words of a tile: [0..2] right edge, bit y set when own pixel
-// (T-1, y) equals the right neighbour's (0, y + d), d = -1, 0, +1; [3..5]
-// bottom edge, bit x for own (x, T-1) and the lower neighbour's (x + d, 0);
-// [6] bit 0: bottom-right corner pair, bit 1: bottom-left corner pair.
+// Seam item of a tile: bits 0-7 own record, 8-14 the neighbour's border
+// offset (its record array index), 16-18 neighbour direction (kRel*).
 
 // Run-log entry: bits 0-7 record, 8-13 x, 14-19 y, 20-26 length.
 __device__ __forceinline__ uint32_t pending_entry(int rec, int x, int y,
@@ -84,10 +82,6 @@ struct __align__(16) WarpSmem {
     uint32_t listed[T];            // per row: listed pixels
     uint32_t cont[T];              // per row: listed run continuations
     int16_t img[kHaloW * kHaloW];  // tile + halo, -1 outside the image
-};
-
-struct __align__(16) ResolveSmem {
-    uint8_t final_flags[kSlots];
 };
 
 struct TileGeom {
@@ -486,7 +480,7 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
     }
     __syncwarp();
 
-    // -- phase F: border records, seam equalities ------------------------------
+    // -- phase F: border records, seam items -----------------------------------
     uint8_t* border = a.border + item * kSlots;
     auto record_of = [&](int x, int y) -> uint32_t {
         if (!((sm.listed[y] >> x) & 1u)) {
@@ -501,56 +495,82 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
         const uint32_t r1 = (w >> kRecShift) & 0xFFu;
         return r1 ? r1 - 1u : kNoRecord;
     };
-    if (lane < g.tw) {
-        border[lane] = static_cast<uint8_t>(record_of(lane, 0));
-        border[T + lane] = static_cast<uint8_t>(record_of(lane, g.th - 1));
-    }
-    if (lane < g.th) {
-        border[2 * T + lane] = static_cast<uint8_t>(record_of(0, lane));
-        border[3 * T + lane] = static_cast<uint8_t>(record_of(g.tw - 1, lane));
-    }
     // Staged pixel (x, y) of the tile, x and y in -1 .. T.
     auto px = [&](int x, int y) -> int {
         return sm.img[(y + 1) * kHaloW + x + 1];
     };
-    const bool has_right = g.x0 + T < width;     // implies tw == T
-    const bool has_below = g.y0 + T < height;    // implies th == T
-    uint32_t eqw[kSeamWords];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const int y = lane;
-        const int y2 = y + d - 1;
-        const bool er = has_right && y < g.th && y2 >= 0 && y2 < g.th &&
-                        px(T - 1, y) == px(T, y2);
-        eqw[d] = __ballot_sync(~0u, er);
+    // Seam items: every equal pair across a seam with a live pixel on this
+    // side, as (own record, neighbour direction, neighbour border offset).
+    // Pairs live on both sides are listed by both tiles; uniting twice is
+    // harmless.  Corner pairs are listed by the top and bottom rows.
+    uint32_t* items = a.seam_items + item * kSeamCap;
+    int nitems = 0;
+    auto emit = [&](bool ok, uint32_t rec, int dir, int off) {
+        const uint32_t bal = __ballot_sync(~0u, ok);
+        if (ok) {
+            items[nitems + __popc(bal & lt_mask)] =
+                rec | (static_cast<uint32_t>(off) << 8) |
+                (static_cast<uint32_t>(dir) << 16);
+        }
+        nitems += __popc(bal);
+    };
+    {
         const int x = lane;
-        const int x2 = x + d - 1;
-        const bool eb = has_below && x < g.tw && x2 >= 0 && x2 < g.tw &&
-                        px(x, T - 1) == px(x2, T);
-        eqw[3 + d] = __ballot_sync(~0u, eb);
+        const bool in_row = x < g.tw;
+        const uint32_t rt = in_row ? record_of(x, 0) : kNoRecord;
+        const uint32_t rb = in_row ? record_of(x, g.th - 1) : kNoRecord;
+        if (in_row) {
+            border[x] = static_cast<uint8_t>(rt);
+            border[T + x] = static_cast<uint8_t>(rb);
+        }
+        const bool live_t = rt < static_cast<uint32_t>(kSlots);
+        const bool live_b = rb < static_cast<uint32_t>(kSlots) &&
+                            g.th == T && g.y0 + T < height;
+        const int vt = px(x, 0);
+        const int vb = px(x, T - 1);
+#pragma unroll
+        for (int d = -1; d <= 1; ++d) {
+            const int x2 = x + d;
+            // Top row: neighbour row -1 of the top, top-left or top-right tile.
+            const int dir_t = x2 < 0 ? kRelTopLeft
+                                     : (x2 >= T ? kRelTopRight : kRelTop);
+            const int off_t = T + (x2 < 0 ? T - 1 : (x2 >= T ? 0 : x2));
+            emit(live_t && px(x2, -1) == vt, rt, dir_t, off_t);
+            // Bottom row: neighbour row T of the lower tiles.
+            const int dir_b = x2 < 0 ? kRelBottomLeft
+                                     : (x2 >= T ? kRelBottomRight : kRelBottom);
+            const int off_b = x2 < 0 ? T - 1 : (x2 >= T ? 0 : x2);
+            emit(live_b && px(x2, T) == vb, rb, dir_b, off_b);
+        }
     }
     {
-        uint32_t corners = 0u;
-        if (has_right && has_below && px(T - 1, T - 1) == px(T, T)) {
-            corners |= 1u;
+        const int y = lane;
+        const bool in_col = y < g.th;
+        const uint32_t rl = in_col ? record_of(0, y) : kNoRecord;
+        const uint32_t rr = in_col ? record_of(g.tw - 1, y) : kNoRecord;
+        if (in_col) {
+            border[2 * T + y] = static_cast<uint8_t>(rl);
+            border[3 * T + y] = static_cast<uint8_t>(rr);
         }
-        if (g.x0 > 0 && has_below && px(0, T - 1) == px(-1, T)) {
-            corners |= 2u;
-        }
-        eqw[6] = corners;
-        eqw[7] = 0u;
-    }
-    uint32_t mine = 0u;
+        const bool live_l = rl < static_cast<uint32_t>(kSlots);
+        const bool live_r = rr < static_cast<uint32_t>(kSlots) &&
+                            g.tw == T && g.x0 + T < width;
+        const int vl = px(0, y);
+        const int vr = px(T - 1, y);
 #pragma unroll
-    for (int k = 0; k < kSeamWords; ++k) {
-        if (lane == k) mine = eqw[k];
-    }
-    if (lane < kSeamWords) {
-        a.seam_eq[item * kSeamWords + lane] = mine;
+        for (int d = -1; d <= 1; ++d) {
+            const int y2 = y + d;
+            const bool inside = y2 >= 0 && y2 < g.th;   // corners: rows above
+            emit(live_l && inside && px(-1, y2) == vl, rl, kRelLeft,
+                 3 * T + y2);
+            emit(live_r && inside && px(T, y2) == vr, rr, kRelRight,
+                 2 * T + y2);
+        }
     }
     if (lane == 0) {
         a.fragment_count[item] = static_cast<uint16_t>(min(nrec, kSlots));
         a.pending_count[item] = static_cast<uint32_t>(nlog);
+        a.seam_count[item] = static_cast<uint32_t>(nitems);
     }
     if (err) {
         raise_error(a.header, err, static_cast<uint32_t>(item));
@@ -558,154 +578,198 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
 }
 
 // ---------------------------------------------------------------------------
-// Seam pass (one warp, the seams one tile owns)
+// Seam and resolve passes: one warp per 32 consecutive tiles, work flattened
+// over the tiles so the global round trips of many tiles overlap.
 // ---------------------------------------------------------------------------
 
-// Joins the border pixel with record r1 of tile g1 to the equal pixel with
-// record r2 of tile g2.
-__device__ __forceinline__ void seam_join(const Arena& a, int64_t g1,
-                                          uint32_t r1, int64_t g2,
-                                          uint32_t r2, uint32_t& err) {
-    if (r1 == kNoRecord || r2 == kNoRecord) {
-        err = kErrInvariant;   // equal across a seam, yet no seam zone
-        return;
+// Exclusive prefix of `v` over the warp; `total` receives the sum.
+__device__ __forceinline__ uint32_t warp_prefix(uint32_t v, uint32_t& total) {
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t n = __shfl_up_sync(~0u, incl, o);
+        if (lane >= o) incl += n;
     }
-    if ((r1 != kDeadRecord && r1 >= static_cast<uint32_t>(kSlots)) ||
-        (r2 != kDeadRecord && r2 >= static_cast<uint32_t>(kSlots))) {
-        err = kErrRecordRange;
-        return;
+    total = __shfl_sync(~0u, incl, 31);
+    return incl - v;
+}
+
+// The lane whose [excl, excl + count) range holds flat index f (all lanes
+// call it together; f may differ per lane).
+__device__ __forceinline__ int owner_of(uint32_t excl, uint32_t f) {
+    int lo = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+        const uint32_t probe = __shfl_sync(~0u, excl, lo + step);
+        if (probe <= f) lo += step;
     }
-    if (r1 == kDeadRecord && r2 == kDeadRecord) {
-        return;
-    }
-    const int f1 = static_cast<int>(g1 * kSlots + r1);
-    const int f2 = static_cast<int>(g2 * kSlots + r2);
-    if (r1 == kDeadRecord) {
-        global_or(a.parent, a.bits, f2, kDead, err);
-    } else if (r2 == kDeadRecord) {
-        global_or(a.parent, a.bits, f1, kDead, err);
-    } else {
-        global_union(a.parent, a.bits, f1, f2, err);
+    return lo;
+}
+
+__device__ __forceinline__ int64_t neighbour_tile(int64_t g, int dir,
+                                                  int64_t tiles_x) {
+    switch (dir) {
+        case kRelLeft: return g - 1;
+        case kRelTop: return g - tiles_x;
+        case kRelTopLeft: return g - tiles_x - 1;
+        case kRelTopRight: return g - tiles_x + 1;
+        case kRelRight: return g + 1;
+        case kRelBottom: return g + tiles_x;
+        case kRelBottomRight: return g + tiles_x + 1;
+        default: return g + tiles_x - 1;
     }
 }
 
-__device__ __forceinline__ void seam_pass_warp(const Source& src,
-                                               const Arena& a, int64_t item) {
+__device__ __forceinline__ void seam_pass_warp32(const Source& src,
+                                                 const Arena& a,
+                                                 int64_t first) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
-    const uint32_t* eq = a.seam_eq + item * kSeamWords;
-    const uint32_t mine = lane < kSeamWords ? __ldg(eq + lane) : 0u;
-    const uint32_t any = __reduce_or_sync(~0u, mine);
-    if (!any) {
+    const int64_t tile = first + lane;
+    const bool valid = tile < src.total_tiles;
+    const uint32_t count =
+        valid ? min(__ldg(a.seam_count + tile), static_cast<uint32_t>(kSeamCap))
+              : 0u;
+    uint32_t total = 0;
+    const uint32_t excl = warp_prefix(count, total);
+    if (total == 0) {
         return;
     }
-    uint32_t eqw[7];
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-        eqw[k] = __shfl_sync(~0u, mine, k);
+    int64_t tiles_x = 0;
+    if (count) {
+        tiles_x = load_job(src, tile).tiles_x;
     }
     uint32_t err = 0;
-    const PlanImage job = load_job(src, item);
-    const int64_t tiles_x = job.tiles_x;
-    const uint8_t* own = a.border + item * kSlots;
-    if (eqw[0] | eqw[1] | eqw[2]) {
-        const int64_t ng = item + 1;
-        const uint8_t* nb = a.border + ng * kSlots;
-        const int y = lane;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            if ((eqw[d] >> y) & 1u) {
-                seam_join(a, item, __ldg(own + 3 * T + y), ng,
-                          __ldg(nb + 2 * T + y + d - 1), err);
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t f = base + static_cast<uint32_t>(lane);
+        const int owner = owner_of(excl, f);
+        const int64_t g = first + owner;
+        const int64_t tx = __shfl_sync(~0u, tiles_x, owner);
+        const uint32_t j = f - __shfl_sync(~0u, excl, owner);
+        if (f < total) {
+            const uint32_t it = __ldcg(a.seam_items + g * kSeamCap + j);
+            const uint32_t rec = it & 0xFFu;
+            const int off = static_cast<int>((it >> 8) & 0x7Fu);
+            const int dir = static_cast<int>((it >> 16) & 7u);
+            const int64_t ng = neighbour_tile(g, dir, tx);
+            if (rec >= static_cast<uint32_t>(kSlots) || ng < 0 ||
+                ng >= src.total_tiles) {
+                err = kErrRecordRange;
+                continue;
+            }
+            const uint32_t rn = __ldg(a.border + ng * kSlots + off);
+            const int fo = static_cast<int>(g * kSlots + rec);
+            if (rn == kDeadRecord) {
+                global_or(a.parent, a.bits, fo, kDead, err);
+            } else if (rn < static_cast<uint32_t>(kSlots)) {
+                global_union(a.parent, a.bits, fo,
+                             static_cast<int>(ng * kSlots + rn), err);
+            } else {
+                err = kErrInvariant;   // equal across a seam, no seam zone
             }
         }
-    }
-    if (eqw[3] | eqw[4] | eqw[5]) {
-        const int64_t ng = item + tiles_x;
-        const uint8_t* nb = a.border + ng * kSlots;
-        const int x = lane;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            if ((eqw[3 + d] >> x) & 1u) {
-                seam_join(a, item, __ldg(own + T + x), ng,
-                          __ldg(nb + x + d - 1), err);
-            }
-        }
-    }
-    if (lane == 0 && (eqw[6] & 1u)) {   // own (T-1, T-1), its (0, 0)
-        const int64_t ng = item + tiles_x + 1;
-        seam_join(a, item, __ldg(own + T + T - 1), ng,
-                  __ldg(a.border + ng * kSlots), err);
-    }
-    if (lane == 0 && (eqw[6] & 2u)) {   // own (0, T-1), its (T-1, 0)
-        const int64_t ng = item + tiles_x - 1;
-        seam_join(a, item, __ldg(own + T), ng,
-                  __ldg(a.border + ng * kSlots + T - 1), err);
     }
     if (err) {
-        raise_error(a.header, err, static_cast<uint32_t>(item));
+        raise_error(a.header, err, static_cast<uint32_t>(first));
     }
 }
 
-// ---------------------------------------------------------------------------
-// Resolve pass (one warp, one tile)
-// ---------------------------------------------------------------------------
+struct __align__(16) ResolveSmem {
+    uint8_t final_flags[32][kSlots];
+    uint8_t* maxima[32];
+    uint8_t* minima[32];
+    int64_t out_origin[32];   // offset of the tile's pixel (0, 0)
+    int32_t out_pitch[32];
+    int16_t tw[32];
+    int16_t th[32];
+};
 
-__device__ __forceinline__ void resolve_warp(ResolveSmem& sm,
-                                             const Source& src,
-                                             const Arena& a, int64_t item) {
+__device__ __forceinline__ void resolve_warp32(ResolveSmem& sm,
+                                               const Source& src,
+                                               const Arena& a, int64_t first) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
-    const uint32_t n = a.pending_count[item];
-    if (n == 0u) {
+    const int64_t tile = first + lane;
+    const bool valid = tile < src.total_tiles;
+    const uint32_t n =
+        valid ? min(a.pending_count[tile], static_cast<uint32_t>(kPendingCap))
+              : 0u;
+    const uint32_t k = n ? min(static_cast<uint32_t>(a.fragment_count[tile]),
+                               static_cast<uint32_t>(kSlots))
+                         : 0u;
+    uint32_t total_n = 0;
+    uint32_t total_k = 0;
+    const uint32_t excl_n = warp_prefix(n, total_n);
+    const uint32_t excl_k = warp_prefix(k, total_k);
+    if (total_n == 0) {
         return;
     }
     uint32_t err = 0;
-    const int count = a.fragment_count[item];
-    const int64_t frag_base = item * kSlots;
-    uint32_t any = 0u;
-#pragma unroll
-    for (int i = 0; i < kSlots / 32; ++i) {
-        const int r = lane + 32 * i;
-        bool flip = false;
-        if (r < count) {
-            const int f = static_cast<int>(frag_base + r);
-            const int root = global_find(a.parent, f, err);
+    if (n) {
+        const PlanImage job = load_job(src, tile);
+        const TileGeom g = tile_geom(job, tile - job.tile_base);
+        sm.maxima[lane] = job.maxima;
+        sm.minima[lane] = job.minima;
+        sm.out_origin[lane] =
+            static_cast<int64_t>(g.y0) * job.out_pitch + g.x0;
+        sm.out_pitch[lane] = job.out_pitch;
+        sm.tw[lane] = static_cast<int16_t>(g.tw);
+        sm.th[lane] = static_cast<int16_t>(g.th);
+    }
+    // Component flags of every live fragment of these tiles.
+    uint32_t flipped = 0u;
+    for (uint32_t base = 0; base < total_k; base += 32) {
+        const uint32_t f = base + static_cast<uint32_t>(lane);
+        const int owner = owner_of(excl_k, f);
+        const uint32_t r = f - __shfl_sync(~0u, excl_k, owner);
+        if (f < total_k) {
+            const int fr = static_cast<int>((first + owner) * kSlots + r);
+            const int root = global_find(a.parent, fr, err);
             const uint32_t comp = ld_relaxed(a.bits + root) & 3u;
-            const uint32_t own = (ld_relaxed(a.bits + f) >> kLocalShift) & 3u;
-            flip = comp != own;
-            sm.final_flags[r] = static_cast<uint8_t>(comp);
+            const uint32_t own = (ld_relaxed(a.bits + fr) >> kLocalShift) & 3u;
+            sm.final_flags[owner][r] = static_cast<uint8_t>(comp);
+            if (comp != own) {
+                flipped |= 1u << owner;
+            }
         }
-        any |= __ballot_sync(~0u, flip);
     }
+    flipped = __reduce_or_sync(~0u, flipped);
     __syncwarp();
-    const PlanImage job = load_job(src, item);
-    const TileGeom g = tile_geom(job, item - job.tile_base);
-    const int64_t out_pitch = job.out_pitch;
-    const uint32_t* plog = a.pending + item * kPendingCap;
-    const uint32_t total = min(n, static_cast<uint32_t>(kPendingCap));
-    for (uint32_t e = lane; e < total; e += 32) {
-        const uint32_t ent = __ldcg(plog + e);
-        const int rec = static_cast<int>(ent & 0xFFu);
-        const int x = static_cast<int>((ent >> 8) & 63u);
-        const int y = static_cast<int>((ent >> 14) & 63u);
-        const int len = static_cast<int>((ent >> 20) & 127u);
-        if (rec >= count || x + len > g.tw || y >= g.th || len == 0) {
-            err = kErrRecordRange;
-            continue;
-        }
-        const uint32_t fl = sm.final_flags[rec];
-        const uint8_t mx = (fl & kHasGreater) ? 0 : 255;
-        const uint8_t mn = (fl & kHasSmaller) ? 0 : 255;
-        const int64_t o = (g.y0 + y) * out_pitch + g.x0 + x;
-        for (int k = 0; k < len; ++k) {
-            job.maxima[o + k] = mx;
-            job.minima[o + k] = mn;
+    // The logged runs.
+    for (uint32_t base = 0; base < total_n; base += 32) {
+        const uint32_t e = base + static_cast<uint32_t>(lane);
+        const int owner = owner_of(excl_n, e);
+        const uint32_t j = e - __shfl_sync(~0u, excl_n, owner);
+        const uint32_t kown = __shfl_sync(~0u, k, owner);
+        if (e < total_n) {
+            const uint32_t ent =
+                __ldcg(a.pending + (first + owner) * kPendingCap + j);
+            const uint32_t rec = ent & 0xFFu;
+            const int x = static_cast<int>((ent >> 8) & 63u);
+            const int y = static_cast<int>((ent >> 14) & 63u);
+            const int len = static_cast<int>((ent >> 20) & 127u);
+            if (rec >= kown ||
+                x + len > sm.tw[owner] || y >= sm.th[owner] || len == 0) {
+                err = kErrRecordRange;
+                continue;
+            }
+            const uint32_t fl = sm.final_flags[owner][rec];
+            const uint8_t mx = (fl & kHasGreater) ? 0 : 255;
+            const uint8_t mn = (fl & kHasSmaller) ? 0 : 255;
+            const int64_t o = sm.out_origin[owner] +
+                              static_cast<int64_t>(y) * sm.out_pitch[owner] + x;
+            uint8_t* pmx = sm.maxima[owner] + o;
+            uint8_t* pmn = sm.minima[owner] + o;
+            for (int q = 0; q < len; ++q) {
+                pmx[q] = mx;
+                pmn[q] = mn;
+            }
         }
     }
-    if (lane == 0 && any) {
-        atomicAdd(&a.header->flipped_tiles, 1u);
+    if (lane == 0 && flipped) {
+        atomicAdd(&a.header->flipped_tiles, __popc(flipped));
     }
     if (err) {
-        raise_error(a.header, err, static_cast<uint32_t>(item));
+        raise_error(a.header, err, static_cast<uint32_t>(first));
     }
 }
 

@@ -46,10 +46,10 @@ def test_workspace_bytes():
     c = pkg.workspace_bytes(1024, 1024, 64)
     assert a % 256 == 0 and b > a and c < b
     # 2040x1356 at T=32: 64 x 43 tiles, 128 slots of 9 bytes each, border
-    # records, counters and a pending-run log of up to 32 x 32 entries of
-    # 4 bytes per tile -> about 5.4 bytes per pixel.
+    # records, counters, a run log of up to 32 x 32 entries of 4 bytes and
+    # up to 384 seam items of 4 bytes per tile -> about 7 bytes per pixel.
     w = pkg.workspace_bytes(2040, 1356, 32)
-    assert 2752 * (128 * 9 + 4096) < w < 2040 * 1356 * 5.6
+    assert 2752 * (128 * 9 + 4096 + 1536) < w < 2040 * 1356 * 7.5
     # T=64 keeps no pending log: about 0.6 bytes per pixel.
     assert pkg.workspace_bytes(2040, 1356, 64) < 2040 * 1356 * 0.7
     with pytest.raises(pkg.SparseSeamError) as e:
