@@ -67,7 +67,9 @@ typedef enum ss_status {
                                       error_flag 3) */
     SS_ERR_SPIN_LIMIT = 10,        /* a bounded device loop gave up */
     SS_ERR_WORKSPACE_UNINITIALIZED = 11, /* ss_workspace_init was not run */
-    SS_ERR_HOST_ALLOC = 12         /* host-side allocation failed */
+    SS_ERR_HOST_ALLOC = 12,        /* host-side allocation failed */
+    SS_ERR_EXCEEDS_STATIC_SCRATCH = 13 /* the image needs more scratch than
+                                          ss_extrema_static_scratch holds */
 } ss_status;
 
 /* Human-readable name of a status code (static storage). */
@@ -127,6 +129,28 @@ typedef struct ss_stats {
  * (harness/configuration_study/sparse_config_benchmark_v0_8.cu:17-30). */
 ss_status ss_set_kernel_config(int tile, int warps);
 ss_status ss_get_kernel_config(int tile, int* warps);
+
+/* Zero-allocation form of ss_extrema, for callers that cannot allocate
+ * device memory (code that must not enter the allocator: another
+ * allocator's callback, a latency-critical loop, a plug-in whose host owns
+ * every device allocation).  No counterpart in the reference, which always
+ * allocates per image.  The route's scratch is a fixed 32 MiB array inside
+ * the library, held on every GPU that loads it until the process exits; this
+ * call allocates nothing (no cudaMalloc, no allocating library routine).
+ * Limits: images whose ss_workspace_bytes exceeds 32 MiB are rejected with
+ * SS_ERR_EXCEEDS_STATIC_SCRATCH (at T = 32 about 4.6 Mpixel, e.g. 2040 x 1356;
+ * at T = 64 about 50 Mpixel).  The first call on a device sets the array up
+ * (looks up its device address with the device current, clears it, waits for
+ * the clear on `stream`); make that first call before any stream capture.
+ * Every call shares the one array and it keeps the previous call's contents,
+ * so each call clears what must start at zero; calls that overlap on the GPU
+ * (other streams, other host threads) race and must be serialised by the
+ * caller.  Device-side invariant failures are recorded in the array's header
+ * and are not reported by this entry point. */
+ss_status ss_extrema_static_scratch(const uint8_t* d_image, int width,
+                                    int height, int pitch, int tile,
+                                    uint8_t* d_maxima, uint8_t* d_minima,
+                                    int out_pitch, void* stream);
 
 /* Synchronises `stream`, copies the status header (and, if `stats` is not
  * NULL, the statistics) to the host and clears the device error word.

@@ -47,6 +47,7 @@ STATUS = {
     10: "SS_ERR_SPIN_LIMIT",
     11: "SS_ERR_WORKSPACE_UNINITIALIZED",
     12: "SS_ERR_HOST_ALLOC",
+    13: "SS_ERR_EXCEEDS_STATIC_SCRATCH",
 }
 
 
@@ -107,6 +108,8 @@ SIGNATURES = {
     "ss_extrema_batch_pass": (_I, [_VP, _VP, _SZ, _I, _I, _VP, _SZ, _VP]),
     "ss_set_kernel_config": (_I, [_I, _I]),
     "ss_get_kernel_config": (_I, [_I, ctypes.POINTER(_I)]),
+    "ss_extrema_static_scratch": (_I, [_VP, _I, _I, _I, _I, _VP, _VP, _I,
+                                       _VP]),
 }
 
 

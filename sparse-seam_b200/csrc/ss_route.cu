@@ -783,6 +783,8 @@ const char* ss_status_string(ss_status status) {
         case SS_ERR_WORKSPACE_UNINITIALIZED:
             return "SS_ERR_WORKSPACE_UNINITIALIZED";
         case SS_ERR_HOST_ALLOC: return "SS_ERR_HOST_ALLOC";
+        case SS_ERR_EXCEEDS_STATIC_SCRATCH:
+            return "SS_ERR_EXCEEDS_STATIC_SCRATCH";
     }
     return "SS_ERR_UNKNOWN";
 }
@@ -1097,6 +1099,88 @@ ss_status ss_extrema_batch_pass(const void* h_plan, const void* d_plan,
     }
     return batch_passes(h_plan, d_plan, plan_bytes, persistent, d_workspace,
                         workspace_bytes, stream, pass);
+}
+
+// ---------------------------------------------------------------------------
+// Zero-allocation form
+// ---------------------------------------------------------------------------
+
+// Some callers cannot allocate device memory: code that runs where the
+// allocator must not be entered (inside another allocator's callback, a
+// latency-critical loop that may not block on cudaMalloc), or a plug-in whose
+// host owns every device allocation.  For them the route's scratch lives in
+// this fixed array instead of a caller-provided workspace.  Every GPU that
+// loads the library holds it until the process exits.
+constexpr size_t kStaticScratchBytes = static_cast<size_t>(32) << 20;
+static __device__ __align__(256) unsigned char
+    g_static_scratch[kStaticScratchBytes];
+
+static std::mutex g_static_mutex;
+static void* g_static_address[256] = {};   // per device, set on first use
+
+ss_status ss_extrema_static_scratch(const uint8_t* d_image, int width,
+                                    int height, int pitch, int tile,
+                                    uint8_t* d_maxima, uint8_t* d_minima,
+                                    int out_pitch, void* stream) {
+    if (!d_image || !d_maxima || !d_minima || width <= 0 || height <= 0 ||
+        pitch < width || out_pitch < width) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    if (!tile_ok(tile)) {
+        return SS_ERR_UNSUPPORTED_TILE;
+    }
+    const int64_t tiles = tiles_of(width, height, tile);
+    size_t needed = 0;
+    if (!workspace_size(tiles, tile, &needed)) {
+        return SS_ERR_TOO_LARGE;
+    }
+    if (needed > kStaticScratchBytes) {
+        return SS_ERR_EXCEEDS_STATIC_SCRATCH;
+    }
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
+        return SS_ERR_CUDA;
+    }
+    if (device < 0 || device >= 256) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    void* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_static_mutex);
+        if (!g_static_address[device]) {
+            // First use on this device (which is current): the array's
+            // device address, then a full clear and the status header.  The
+            // set-up is waited for, so later calls on any stream see it.
+            void* address = nullptr;
+            if (cudaGetSymbolAddress(&address, g_static_scratch) !=
+                    cudaSuccess ||
+                !address) {
+                return SS_ERR_CUDA;
+            }
+            const ss_status init =
+                ss_workspace_init(address, kStaticScratchBytes, stream);
+            if (init != SS_OK) {
+                return init;
+            }
+            if (cudaStreamSynchronize(st) != cudaSuccess) {
+                return SS_ERR_CUDA;
+            }
+            g_static_address[device] = address;
+        }
+        scratch = g_static_address[device];
+    }
+    // The array keeps the previous call's contents.  What this call needs at
+    // zero: the error word and the seam-pair counters of this geometry.
+    Header* header = static_cast<Header*>(scratch);
+    if (cudaMemsetAsync(&header->error, 0, 2 * sizeof(uint32_t), st) !=
+            cudaSuccess ||
+        cudaMemsetAsync(static_cast<char*>(scratch) + sizeof(Header), 0,
+                        static_cast<size_t>(tiles) * 16, st) != cudaSuccess) {
+        return SS_ERR_CUDA;
+    }
+    return ss_extrema(d_image, width, height, pitch, tile, d_maxima, d_minima,
+                      out_pitch, scratch, kStaticScratchBytes, stream);
 }
 
 // ---------------------------------------------------------------------------
