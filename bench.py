@@ -79,34 +79,48 @@ def parse_args():
 # ---------------------------------------------------------------------------
 
 class Dist:
-    def __init__(self):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE).
+
+    Only timing crosses ranks (a barrier and a max over the measured times);
+    the images are independent, so no collective touches the data path.
+    `backend` is "nccl" on GPUs; the CPU tests use "gloo".
+    """
+
+    def __init__(self, backend: str = "nccl"):
         import torch
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
         self.pg = False
         if self.world > 1:
             import datetime
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
+            kwargs = {}
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                kwargs["device_id"] = torch.device("cuda", self.local)
             dist.init_process_group(
-                "nccl", timeout=datetime.timedelta(seconds=300),
-                device_id=torch.device("cuda", self.local))
+                backend, timeout=datetime.timedelta(seconds=300), **kwargs)
             self.pg = True
 
     def barrier(self):
         if self.pg:
             import torch
             import torch.distributed as dist
-            dist.barrier(device_ids=[self.local])
-            torch.cuda.synchronize()
+            if self.backend == "nccl":
+                dist.barrier(device_ids=[self.local])
+                torch.cuda.synchronize()
+            else:
+                dist.barrier()
 
     def max(self, value: float) -> float:
         if not self.pg:
             return value
         import torch
         import torch.distributed as dist
-        t = torch.tensor([value], dtype=torch.float64, device="cuda")
+        device = "cuda" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([value], dtype=torch.float64, device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
@@ -196,6 +210,11 @@ class ClockSampler:
 
 def corpus_shapes(n_large: int, n_small: int):
     return [(1356, 2040)] * n_large + [(321, 481)] * n_small
+
+
+def corpus_seed_base(rank: int) -> int:
+    """Each rank (replica) processes its own corpus."""
+    return 7919 * rank
 
 
 def make_corpus(n_large: int, n_small: int, seed_base: int, device,
@@ -381,8 +400,8 @@ def main():
     torch.cuda.set_device(device)
     tile = args.tile
 
-    images = make_corpus(args.large, args.small, 7919 * dist.rank, device,
-                         args.levels)
+    images = make_corpus(args.large, args.small, corpus_seed_base(dist.rank),
+                         device, args.levels)
     pixels = sum(im.numel() for im in images)
     maxs = [torch.empty_like(im) for im in images]
     mins = [torch.empty_like(im) for im in images]
