@@ -227,6 +227,121 @@ ss_status ss_extrema_batch_pass(const void* h_plan, const void* d_plan,
                                 void* d_workspace, size_t workspace_bytes,
                                 void* stream);
 
+/* Per-call launch choices: the knobs of the batch autotuner.  None of them
+ * changes the masks.  No counterpart in the reference, whose tile, classify
+ * threads and flatten launch are compile-time constants
+ * (harness/configuration_study/sparse_config_benchmark_v0_8.cu:17-30). */
+typedef struct ss_launch {
+    int32_t warps;       /* kernel family for the plan's tile, as in
+                          * ss_set_kernel_config; 0 = the tile's current
+                          * default */
+    int32_t persistent;  /* 0 grid schedule, 1 persistent work queue */
+    int32_t group;       /* row-scan seam and resolve passes: tiles per warp,
+                          * 1, 2, 4, 8, 16 or 32; 0 = chosen from the tile
+                          * count (one tile per warp for small launches, up to
+                          * 32 for large ones) */
+    int32_t passes;      /* passes to enqueue (1 tile, 4 seam, 2 resolve,
+                          * enqueued in that order); 0 = all */
+} ss_launch;
+
+/* ss_extrema_batch with explicit launch choices (NULL = all defaults). */
+ss_status ss_extrema_batch_launch(const void* h_plan, const void* d_plan,
+                                  size_t plan_bytes, const ss_launch* launch,
+                                  void* d_workspace, size_t workspace_bytes,
+                                  void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* Serving: a continuous-batching request loop on one GPU.                 */
+/* ---------------------------------------------------------------------- */
+/* No counterpart in the reference, whose harness runs one image at a time
+ * (harness/primary/gpu_common_v0_6.cu:137-206).  A server owns, for its
+ * lifetime, a device pool for request buffers and `inflight` batch slots
+ * (a stream, a DSU workspace for `batch_tiles` tiles and a plan buffer
+ * each).  A worker thread admits submitted requests in arrival order as pool
+ * memory frees up (admission by HBM footprint: image plus two masks), copies
+ * their images in on a copy stream, and whenever a slot is free launches
+ * every admitted request not yet launched as one batch (ss_extrema_batch),
+ * so requests arriving while others run join the next batch and batches
+ * overlap on the device.  Each slot's stream then copies the masks out,
+ * reads the batch's device status and frees the requests' pool memory.
+ * Masks are the same as ss_extrema's on each image alone.  Thread-safe:
+ * any thread may submit and poll. */
+
+#define SS_REQUEST_DEVICE 1u  /* image and masks are device pointers owned by
+                               * the caller: no pool memory, no copies */
+
+typedef struct ss_request {
+    const uint8_t* image;   /* host (pinned for overlap) or device pointer */
+    uint8_t* maxima;
+    uint8_t* minima;
+    int32_t width;
+    int32_t height;
+    int32_t pitch;
+    int32_t out_pitch;
+    uint32_t flags;         /* SS_REQUEST_* */
+    uint32_t reserved;
+    uint64_t user;          /* returned in the completion */
+} ss_request;
+
+typedef struct ss_completion {
+    uint64_t ticket;
+    uint64_t user;
+    int32_t status;         /* SS_OK or the batch's device failure */
+    int32_t batch_images;   /* requests in the batch that carried it */
+    int64_t submit_ns;      /* CLOCK_MONOTONIC nanoseconds */
+    int64_t admit_ns;       /* pool memory granted, copy-in enqueued */
+    int64_t launch_ns;      /* batch enqueued */
+    int64_t done_ns;        /* masks in the caller's buffers */
+} ss_completion;
+
+typedef struct ss_server_config {
+    int32_t device;           /* CUDA device ordinal */
+    int32_t tile;             /* 16, 32 or 64 */
+    int32_t persistent;       /* batch schedule, as in ss_extrema_batch */
+    int32_t inflight;         /* batch slots, 1..16 */
+    int32_t max_batch_images; /* requests per batch, >= 1 */
+    int32_t reserved;
+    int64_t batch_tiles;      /* tile capacity of one batch's workspace */
+    uint64_t pool_bytes;      /* device bytes for request images and masks */
+} ss_server_config;
+
+typedef struct ss_server_stats {
+    uint64_t submitted;
+    uint64_t completed;
+    uint64_t batches;
+    uint64_t pixels;               /* of completed requests */
+    uint64_t pool_bytes;
+    uint64_t pool_high_water;      /* most pool bytes in use at once */
+    uint32_t max_batch_images_seen;
+    uint32_t inflight_high_water;  /* most batches on the device at once */
+} ss_server_stats;
+
+typedef struct ss_server ss_server;
+
+/* Allocates the pool and slots on `config->device` and starts the worker.
+ * Fails with SS_ERR_INVALID_VALUE / SS_ERR_UNSUPPORTED_TILE on a bad config
+ * (checked before any CUDA call), SS_ERR_TOO_LARGE if `batch_tiles` exceeds
+ * the workspace's index range, SS_ERR_CUDA on allocation failure. */
+ss_status ss_server_create(const ss_server_config* config,
+                           ss_server** server);
+
+/* Queues one request; `ticket` (optional) receives its id.  Rejected at once
+ * with SS_ERR_TOO_LARGE if it can never fit (more tiles than batch_tiles or
+ * more bytes than the pool), SS_ERR_INVALID_VALUE on bad geometry. */
+ss_status ss_server_submit(ss_server* server, const ss_request* request,
+                           uint64_t* ticket);
+
+/* Moves up to `capacity` completions into `out`, waiting up to `timeout_us`
+ * microseconds for the first one (0: no wait).  `count` receives how many. */
+ss_status ss_server_poll(ss_server* server, ss_completion* out, int capacity,
+                         int* count, int timeout_us);
+
+ss_status ss_server_get_stats(ss_server* server, ss_server_stats* stats);
+
+/* Finishes every submitted request, stops the worker and frees the server's
+ * memory.  Completions not yet polled are dropped. */
+void ss_server_destroy(ss_server* server);
+
 #ifdef __cplusplus
 }
 #endif

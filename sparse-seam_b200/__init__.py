@@ -81,6 +81,74 @@ class ImageDesc(ctypes.Structure):
     ]
 
 
+class Launch(ctypes.Structure):
+    """Per-call launch choices (ss_launch): the batch autotuner's knobs."""
+    _fields_ = [
+        ("warps", ctypes.c_int32),
+        ("persistent", ctypes.c_int32),
+        ("group", ctypes.c_int32),
+        ("passes", ctypes.c_int32),
+    ]
+
+
+# Serving loop (ss_server_*).
+class Request(ctypes.Structure):
+    _fields_ = [
+        ("image", ctypes.c_void_p),
+        ("maxima", ctypes.c_void_p),
+        ("minima", ctypes.c_void_p),
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("pitch", ctypes.c_int32),
+        ("out_pitch", ctypes.c_int32),
+        ("flags", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+        ("user", ctypes.c_uint64),
+    ]
+
+
+class Completion(ctypes.Structure):
+    _fields_ = [
+        ("ticket", ctypes.c_uint64),
+        ("user", ctypes.c_uint64),
+        ("status", ctypes.c_int32),
+        ("batch_images", ctypes.c_int32),
+        ("submit_ns", ctypes.c_int64),
+        ("admit_ns", ctypes.c_int64),
+        ("launch_ns", ctypes.c_int64),
+        ("done_ns", ctypes.c_int64),
+    ]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32),
+        ("tile", ctypes.c_int32),
+        ("persistent", ctypes.c_int32),
+        ("inflight", ctypes.c_int32),
+        ("max_batch_images", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("batch_tiles", ctypes.c_int64),
+        ("pool_bytes", ctypes.c_uint64),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_uint64),
+        ("completed", ctypes.c_uint64),
+        ("batches", ctypes.c_uint64),
+        ("pixels", ctypes.c_uint64),
+        ("pool_bytes", ctypes.c_uint64),
+        ("pool_high_water", ctypes.c_uint64),
+        ("max_batch_images_seen", ctypes.c_uint32),
+        ("inflight_high_water", ctypes.c_uint32),
+    ]
+
+    def as_dict(self) -> Dict[str, int]:
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
 _LIB: Optional[ctypes.CDLL] = None
 
 # name -> (restype, argtypes); every symbol include/sparse_seam.h declares.
@@ -110,6 +178,16 @@ SIGNATURES = {
     "ss_get_kernel_config": (_I, [_I, ctypes.POINTER(_I)]),
     "ss_extrema_static_scratch": (_I, [_VP, _I, _I, _I, _I, _VP, _VP, _I,
                                        _VP]),
+    "ss_extrema_batch_launch": (_I, [_VP, _VP, _SZ, ctypes.POINTER(Launch),
+                                     _VP, _SZ, _VP]),
+    "ss_server_create": (_I, [ctypes.POINTER(ServerConfig),
+                              ctypes.POINTER(_VP)]),
+    "ss_server_submit": (_I, [_VP, ctypes.POINTER(Request),
+                              ctypes.POINTER(ctypes.c_uint64)]),
+    "ss_server_poll": (_I, [_VP, ctypes.POINTER(Completion), _I,
+                            ctypes.POINTER(_I), _I]),
+    "ss_server_get_stats": (_I, [_VP, ctypes.POINTER(ServerStats)]),
+    "ss_server_destroy": (None, [_VP]),
 }
 
 
@@ -305,6 +383,20 @@ class BatchPlan:
             self.plan_bytes, 1 if persistent else 0, workspace.ptr,
             workspace.nbytes, _stream_handle(stream))
         _check(st, "ss_extrema_batch")
+
+    def run_launch(self, workspace: Workspace, warps: int = 0,
+                   persistent: bool = False, group: int = 0, passes: int = 0,
+                   stream=None) -> None:
+        """ss_extrema_batch_launch: explicit kernel family (0 = the tile's
+        default), schedule, seam/resolve tiles per warp (0 = automatic) and
+        passes (0 = all)."""
+        launch = Launch(int(warps), 1 if persistent else 0, int(group),
+                        int(passes))
+        st = lib().ss_extrema_batch_launch(
+            self.host_plan.ctypes.data, self.device_plan.data_ptr(),
+            self.plan_bytes, ctypes.byref(launch), workspace.ptr,
+            workspace.nbytes, _stream_handle(stream))
+        _check(st, "ss_extrema_batch_launch")
 
     def run_pass(self, workspace: Workspace, which: int,
                  persistent: bool = False, stream=None) -> None:

@@ -1,0 +1,197 @@
+"""Batch autotuner: per image-size class, the tile, kernel family, schedule and
+seam/resolve grouping that run a batch fastest on this GPU.
+
+The reference fixes its tile size and classify threads at compile time and
+sweeps them with a separate benchmark binary
+(harness/configuration_study/sparse_config_benchmark_v0_8.cu:17-30).  Here the
+choice is made at run time, per size class, by timing candidate launches
+(``ss_extrema_batch_launch``) on a seeded synthetic batch of that class with
+CUDA events.  No choice changes the masks: every candidate's masks are checked
+byte-equal to the first candidate's before its time is accepted.
+
+A class is a range of image areas (pixels).  `TunedBatch` splits a batch by
+class and runs one launch per class with that class's choice.
+"""
+from __future__ import annotations
+
+import importlib
+import json
+from dataclasses import asdict, dataclass
+from typing import Dict, List, Optional, Sequence, Tuple
+
+_pkg = importlib.import_module(__package__)
+
+# Upper bounds (exclusive) of the area classes, in pixels.
+CLASS_BOUNDS = (64 * 64 * 4, 256 * 256, 512 * 512, 1 << 40)
+
+
+def size_class(height: int, width: int) -> int:
+    area = int(height) * int(width)
+    for k, bound in enumerate(CLASS_BOUNDS):
+        if area < bound:
+            return k
+    return len(CLASS_BOUNDS) - 1
+
+
+@dataclass(frozen=True)
+class Choice:
+    tile: int
+    warps: int        # ss_set_kernel_config value (negative: row-scan)
+    persistent: bool
+    group: int        # row-scan seam/resolve tiles per warp, 0 = automatic
+
+    def label(self) -> str:
+        kind = f"rowscan{-self.warps}" if self.warps < 0 else \
+            f"cta{self.warps}"
+        return (f"T{self.tile}-{kind}-{'persistent' if self.persistent else 'grid'}"
+                f"-g{self.group}")
+
+
+def candidates() -> List[Choice]:
+    """Every launch choice the library offers."""
+    out = []
+    for tile, family in _pkg.KERNEL_CONFIGS.items():
+        for warps in family:
+            for persistent in (False, True):
+                groups = (0, 1, 4, 32) if warps < 0 else (0,)
+                for group in groups:
+                    out.append(Choice(tile, warps, persistent, group))
+    # The library's defaults first: they are the comparison baseline.
+    default = [c for c in out if c.tile == 32 and
+               c.warps == _pkg.get_kernel_config(32) and not c.persistent and
+               c.group == 0]
+    return default + [c for c in out if c not in default]
+
+
+@dataclass
+class TuningTable:
+    choices: Dict[int, Choice]
+    timings_ms: Dict[int, Dict[str, float]]
+
+    def choice_for(self, height: int, width: int) -> Choice:
+        return self.choices[size_class(height, width)]
+
+    def to_json(self) -> str:
+        return json.dumps({
+            "class_bounds": list(CLASS_BOUNDS),
+            "choices": {str(k): asdict(v) for k, v in self.choices.items()},
+            "timings_ms": {str(k): v for k, v in self.timings_ms.items()},
+        })
+
+    @staticmethod
+    def from_json(text: str) -> "TuningTable":
+        data = json.loads(text)
+        if list(data["class_bounds"]) != list(CLASS_BOUNDS):
+            raise ValueError("table was tuned for other size classes")
+        return TuningTable(
+            {int(k): Choice(**v) for k, v in data["choices"].items()},
+            {int(k): v for k, v in data.get("timings_ms", {}).items()})
+
+
+def class_sample(k: int, pixels: int, seed: int, device) -> List:
+    """Seeded mixed-generator images whose areas fall in class k."""
+    synth = importlib.import_module(__package__ + ".synth")
+    lo = 0 if k == 0 else CLASS_BOUNDS[k - 1]
+    hi = CLASS_BOUNDS[k] if k + 1 < len(CLASS_BOUNDS) else 2048 * 2048
+    # Side ranges that make most drawn sizes fall in the class.
+    side_lo, side_hi = ((32, 160), (96, 320), (224, 640), (512, 2048))[k]
+    imgs, total, s = [], 0, seed
+    while total < pixels:
+        batch = synth.uneven_batch(64, seed=s, lo=side_lo, hi=side_hi,
+                                   device=device)
+        s += 1
+        for im in batch:
+            a = im.shape[0] * im.shape[1]
+            if max(lo, 1) <= a < hi:
+                imgs.append(im)
+                total += a
+                if total >= pixels:
+                    break
+    return imgs
+
+
+def _time_choice(images, choice: Choice, reps: int, stream):
+    import torch
+    maxs = [torch.empty_like(i) for i in images]
+    mins = [torch.empty_like(i) for i in images]
+    plan = _pkg.BatchPlan(images, maxs, mins, tile=choice.tile, stream=stream)
+    ws = plan.make_workspace(stream=stream)
+    run = lambda: plan.run_launch(ws, warps=choice.warps,       # noqa: E731
+                                  persistent=choice.persistent,
+                                  group=choice.group, stream=stream)
+    with torch.cuda.stream(stream):
+        run()
+        run()
+    ws.read_status(stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        run()
+    e1.record(stream)
+    e1.synchronize()
+    ws.read_status(stream)
+    return e0.elapsed_time(e1) / reps, maxs, mins
+
+
+def tune(pixels_per_class: int = 16 << 20, reps: int = 5, seed: int = 0,
+         device="cuda", classes: Optional[Sequence[int]] = None,
+         choices: Optional[Sequence[Choice]] = None) -> TuningTable:
+    """Times every candidate on a synthetic batch of each class and keeps the
+    fastest.  Raises if any candidate's masks differ from the first's."""
+    import torch
+    stream = torch.cuda.Stream()
+    cands = list(choices) if choices else candidates()
+    picked: Dict[int, Choice] = {}
+    timings: Dict[int, Dict[str, float]] = {}
+    for k in (classes if classes is not None else range(len(CLASS_BOUNDS))):
+        images = class_sample(k, pixels_per_class, seed + 7919 * k, device)
+        ref = None
+        best = None
+        timings[k] = {}
+        for c in cands:
+            ms, mx, mn = _time_choice(images, c, reps, stream)
+            if ref is None:
+                ref = (mx, mn)
+            else:
+                for a, b in zip(ref[0] + ref[1], mx + mn):
+                    if not torch.equal(a, b):
+                        raise RuntimeError(
+                            f"class {k}: {c.label()} changed the masks")
+            timings[k][c.label()] = round(ms, 4)
+            if best is None or ms < best[0]:
+                best = (ms, c)
+        picked[k] = best[1]
+    return TuningTable(picked, timings)
+
+
+class TunedBatch:
+    """A batch split by size class, each part launched with its tuned choice.
+
+    Parts run one after another on one stream, so the whole batch can be
+    captured in one CUDA graph.
+    """
+
+    def __init__(self, images: Sequence, maxima: Sequence, minima: Sequence,
+                 table: TuningTable, stream=None):
+        parts: Dict[Choice, List[int]] = {}
+        for i, im in enumerate(images):
+            parts.setdefault(table.choice_for(*im.shape), []).append(i)
+        self.parts: List[Tuple[Choice, object, object]] = []
+        for choice, idx in sorted(parts.items(), key=lambda kv: kv[0].label()):
+            plan = _pkg.BatchPlan([images[i] for i in idx],
+                                  [maxima[i] for i in idx],
+                                  [minima[i] for i in idx], tile=choice.tile,
+                                  stream=stream)
+            self.parts.append((choice, plan,
+                               plan.make_workspace(stream=stream)))
+
+    def run(self, stream=None) -> None:
+        for choice, plan, ws in self.parts:
+            plan.run_launch(ws, warps=choice.warps,
+                            persistent=choice.persistent, group=choice.group,
+                            stream=stream)
+
+    def read_status(self, stream=None) -> None:
+        for _, _, ws in self.parts:
+            ws.read_status(stream)

@@ -1,6 +1,7 @@
 """Build recipe for the CUDA route library (sm_100a).
 
-Compiles ``csrc/ss_route.cu`` into ``libsparseseam.so`` next to this file with
+Compiles ``csrc/ss_route.cu`` (the route) and ``csrc/ss_server.cu`` (the
+serving loop) into ``libsparseseam.so`` next to this file with
 nvcc.  The library has a plain C ABI (``include/sparse_seam.h``) and links the
 CUDA runtime statically, so it loads into any process on the GPU host, with or
 without PyTorch.
@@ -14,12 +15,13 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 INCLUDE = os.path.join(ROOT, "include")
-SOURCES = [os.path.join(HERE, "csrc", "ss_route.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "ss_route.cu"),
+           os.path.join(HERE, "csrc", "ss_server.cu")]
 DEPENDS = SOURCES + [
-    os.path.join(HERE, "csrc", "ss_device.cuh"),
-    os.path.join(HERE, "csrc", "ss_tile.cuh"),
-    os.path.join(INCLUDE, "sparse_seam.h"),
-]
+    os.path.join(HERE, "csrc", name)
+    for name in ("ss_device.cuh", "ss_tile.cuh", "ss_rowscan.cuh",
+                 "ss_internal.h", "ss_pool.hpp")
+] + [os.path.join(INCLUDE, "sparse_seam.h")]
 LIBRARY = os.path.join(HERE, "libsparseseam.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -101,6 +101,8 @@ struct Source {
     const int32_t* tile_image;   // batch tile -> image map, or nullptr
     PlanImage single;            // the image when images == nullptr
     int64_t total_tiles;
+    int32_t group;               // tiles per warp in the row-scan seam and
+                                 //   resolve passes (power of two, 1..32)
 };
 
 // Device view of the workspace arrays (global tile index g, slot s).

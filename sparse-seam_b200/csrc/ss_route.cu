@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "sparse_seam.h"
+#include "ss_internal.h"
 #include "ss_rowscan.cuh"
 #include "ss_tile.cuh"
 
@@ -468,7 +469,7 @@ rowscan_tile_pass_kernel(Source src, Arena a) {
     }
 }
 
-// Seam and resolve passes: each warp takes 32 consecutive tiles.
+// Seam and resolve passes: each warp takes src.group consecutive tiles.
 template <int NW, bool kPersistent>
 __global__ void __launch_bounds__(NW * 32)
 rowscan_seam_pass_kernel(Source src, Arena a) {
@@ -478,7 +479,7 @@ rowscan_seam_pass_kernel(Source src, Arena a) {
     }
     const int warp = static_cast<int>(threadIdx.x) >> 5;
     const int64_t first =
-        (static_cast<int64_t>(blockIdx.x) * NW + warp) * 32;
+        (static_cast<int64_t>(blockIdx.x) * NW + warp) * src.group;
     if (first < src.total_tiles) {
         rowscan::seam_pass_warp32(src, a, first);
     }
@@ -500,7 +501,7 @@ rowscan_resolve_pass_kernel(Source src, Arena a) {
                 group = atomicAdd(&a.header->resolve_head, 1u);
             }
             group = __shfl_sync(~0u, group, 0);
-            const int64_t first = static_cast<int64_t>(group) * 32;
+            const int64_t first = static_cast<int64_t>(group) * src.group;
             if (first >= src.total_tiles) {
                 break;
             }
@@ -519,7 +520,7 @@ rowscan_resolve_pass_kernel(Source src, Arena a) {
         }
     } else {
         const int64_t first =
-            (static_cast<int64_t>(blockIdx.x) * NW + warp) * 32;
+            (static_cast<int64_t>(blockIdx.x) * NW + warp) * src.group;
         if (first < src.total_tiles) {
             rowscan::resolve_warp32(sm[warp], src, a, first);
         }
@@ -715,41 +716,87 @@ static int persistent_grid(Kernel k, int threads) {
     return grid;
 }
 
-static ss_status launch_route(const Config& cfg, const Source& src,
+// Streaming multiprocessors of the current device (cached per device).
+static int sm_count() {
+    static std::atomic<int> cache[64] = {};
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
+        return 0;
+    }
+    if (device >= 0 && device < 64) {
+        const int c = cache[device].load();
+        if (c > 0) {
+            return c;
+        }
+    }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) !=
+        cudaSuccess) {
+        return 0;
+    }
+    if (device >= 0 && device < 64) {
+        cache[device].store(sms);
+    }
+    return sms;
+}
+
+// Tiles per warp of the row-scan seam and resolve passes: the smallest power
+// of two (at most 32) that keeps the grid within 64 warps per SM.  Small
+// launches (one image) get one tile per warp, so each warp's chain of
+// dependent global loads is short; large batches get 32, so one warp
+// overlaps the round trips of many tiles.
+static int later_group(int64_t tiles) {
+    const int64_t target = static_cast<int64_t>(std::max(1, sm_count())) * 64;
+    int group = 1;
+    while (group < 32 && tiles > static_cast<int64_t>(group) * target) {
+        group *= 2;
+    }
+    return group;
+}
+
+bool workspace_bytes_for_tiles(int64_t tiles, int tile, size_t* bytes) {
+    return tile_ok(tile) && tiles >= 0 && workspace_size(tiles, tile, bytes);
+}
+
+static ss_status launch_route(const Config& cfg, const Source& src_in,
                               const Arena& arena, int persistent,
-                              cudaStream_t stream, int passes = 7) {
-    if (src.total_tiles == 0) {
+                              cudaStream_t stream, int passes = 7,
+                              int group = 0) {
+    if (src_in.total_tiles == 0) {
         return SS_OK;
     }
-    const int threads = (cfg.warps < 0 ? -cfg.warps : cfg.warps) * 32;
+    Source src = src_in;
+    const int nw = cfg.warps < 0 ? -cfg.warps : cfg.warps;
+    const int threads = nw * 32;
+    // Tiles per CTA of the passes after the tile pass.
+    int later_per_cta = cfg.later_per_cta;
+    src.group = 32;
+    if (cfg.seam_pass) {
+        src.group = group > 0 ? group : later_group(src.total_tiles);
+        later_per_cta = src.group * nw;
+    }
     const int p = persistent ? 1 : 0;
-    unsigned grid1;
-    unsigned grid2;
+    const int64_t ctas1 =
+        (src.total_tiles + cfg.items_per_cta - 1) / cfg.items_per_cta;
+    const int64_t ctas2 =
+        (src.total_tiles + later_per_cta - 1) / later_per_cta;
+    unsigned grid1 = static_cast<unsigned>(ctas1);
+    unsigned grid2 = static_cast<unsigned>(ctas2);
     if (p) {
         const int g1 = persistent_grid(cfg.tile_pass[1], threads);
         const int g2 = persistent_grid(cfg.resolve_pass[1], threads);
         if (g1 <= 0 || g2 <= 0) {
             return SS_ERR_CUDA;
         }
-        const int64_t ctas1 = (src.total_tiles + cfg.items_per_cta - 1) /
-                              cfg.items_per_cta;
-        const int64_t ctas2 = (src.total_tiles + cfg.later_per_cta - 1) /
-                              cfg.later_per_cta;
         grid1 = static_cast<unsigned>(std::min<int64_t>(g1, ctas1));
         grid2 = static_cast<unsigned>(std::min<int64_t>(g2, ctas2));
-    } else {
-        grid1 = static_cast<unsigned>(
-            (src.total_tiles + cfg.items_per_cta - 1) / cfg.items_per_cta);
-        grid2 = static_cast<unsigned>(
-            (src.total_tiles + cfg.later_per_cta - 1) / cfg.later_per_cta);
     }
     if (passes & 1) {
         cfg.tile_pass[p]<<<grid1, threads, 0, stream>>>(src, arena);
     }
     if ((passes & 4) && cfg.seam_pass) {
-        const unsigned grid_seam = static_cast<unsigned>(
-            (src.total_tiles + cfg.later_per_cta - 1) / cfg.later_per_cta);
-        cfg.seam_pass<<<grid_seam, threads, 0, stream>>>(src, arena);
+        cfg.seam_pass<<<static_cast<unsigned>(ctas2), threads, 0, stream>>>(
+            src, arena);
     }
     if (passes & 2) {
         cfg.resolve_pass[p]<<<grid2, threads, 0, stream>>>(src, arena);
@@ -1039,9 +1086,13 @@ ss_status ss_batch_plan_fill(const ss_image_desc* descs, int count, int tile,
 static ss_status batch_passes(const void* h_plan, const void* d_plan,
                               size_t plan_bytes, int persistent,
                               void* d_workspace, size_t workspace_bytes,
-                              void* stream, int passes) {
+                              void* stream, int passes, int warps = 0,
+                              int group = 0) {
     if (!h_plan || !d_plan || !d_workspace ||
         plan_bytes < sizeof(PlanHeader)) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    if (group != 0 && (group < 0 || group > 32 || (group & (group - 1)))) {
         return SS_ERR_INVALID_VALUE;
     }
     if (reinterpret_cast<uintptr_t>(d_workspace) % 256 != 0 ||
@@ -1067,9 +1118,10 @@ static ss_status batch_passes(const void* h_plan, const void* d_plan,
         !layout_for(ph->total_tiles, ph->tile, workspace_bytes, &L)) {
         return SS_ERR_WORKSPACE_TOO_SMALL;
     }
-    const Config* cfg = default_config(ph->tile);
+    const Config* cfg =
+        warps ? find_config(ph->tile, warps) : default_config(ph->tile);
     if (!cfg) {
-        return SS_ERR_UNSUPPORTED_TILE;
+        return warps ? SS_ERR_INVALID_VALUE : SS_ERR_UNSUPPORTED_TILE;
     }
     const PlanHeader* dph = static_cast<const PlanHeader*>(d_plan);
     Source src{};
@@ -1079,7 +1131,7 @@ static ss_status batch_passes(const void* h_plan, const void* d_plan,
     src.total_tiles = ph->total_tiles;
     return launch_route(*cfg, src, arena_at(d_workspace, L),
                         persistent ? 1 : 0,
-                        static_cast<cudaStream_t>(stream), passes);
+                        static_cast<cudaStream_t>(stream), passes, group);
 }
 
 ss_status ss_extrema_batch(const void* h_plan, const void* d_plan,
@@ -1088,6 +1140,22 @@ ss_status ss_extrema_batch(const void* h_plan, const void* d_plan,
                            void* stream) {
     return batch_passes(h_plan, d_plan, plan_bytes, persistent, d_workspace,
                         workspace_bytes, stream, 7);
+}
+
+ss_status ss_extrema_batch_launch(const void* h_plan, const void* d_plan,
+                                  size_t plan_bytes, const ss_launch* launch,
+                                  void* d_workspace, size_t workspace_bytes,
+                                  void* stream) {
+    ss_launch l{};
+    if (launch) {
+        l = *launch;
+    }
+    if (l.passes < 0 || l.passes > 7) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    return batch_passes(h_plan, d_plan, plan_bytes, l.persistent ? 1 : 0,
+                        d_workspace, workspace_bytes, stream,
+                        l.passes ? l.passes : 7, l.warps, l.group);
 }
 
 ss_status ss_extrema_batch_pass(const void* h_plan, const void* d_plan,

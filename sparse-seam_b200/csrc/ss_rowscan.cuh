@@ -578,8 +578,9 @@ __device__ __forceinline__ void tile_pass_warp(WarpSmem& sm, const Source& src,
 }
 
 // ---------------------------------------------------------------------------
-// Seam and resolve passes: one warp per 32 consecutive tiles, work flattened
-// over the tiles so the global round trips of many tiles overlap.
+// Seam and resolve passes: one warp per `group` consecutive tiles (1..32,
+// chosen by the launch so the grid fills the GPU), work flattened over the
+// tiles so the global round trips of many tiles overlap.
 // ---------------------------------------------------------------------------
 
 // Exclusive prefix of `v` over the warp; `total` receives the sum.
@@ -626,7 +627,7 @@ __device__ __forceinline__ void seam_pass_warp32(const Source& src,
                                                  int64_t first) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
     const int64_t tile = first + lane;
-    const bool valid = tile < src.total_tiles;
+    const bool valid = lane < src.group && tile < src.total_tiles;
     const uint32_t count =
         valid ? min(__ldg(a.seam_count + tile), static_cast<uint32_t>(kSeamCap))
               : 0u;
@@ -689,7 +690,7 @@ __device__ __forceinline__ void resolve_warp32(ResolveSmem& sm,
                                                const Arena& a, int64_t first) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
     const int64_t tile = first + lane;
-    const bool valid = tile < src.total_tiles;
+    const bool valid = lane < src.group && tile < src.total_tiles;
     const uint32_t n =
         valid ? min(a.pending_count[tile], static_cast<uint32_t>(kPendingCap))
               : 0u;
