@@ -765,6 +765,11 @@ static ss_status launch_route(const Config& cfg, const Source& src_in,
     if (src_in.total_tiles == 0) {
         return SS_OK;
     }
+    // The status reports this call's launches only: drop a result left in
+    // the thread's last-error slot by earlier runtime calls (a query that
+    // answered cudaErrorNotReady, for instance).  Sticky errors still fail
+    // the launches below.
+    (void)cudaGetLastError();
     Source src = src_in;
     const int nw = cfg.warps < 0 ? -cfg.warps : cfg.warps;
     const int threads = nw * 32;

@@ -215,7 +215,7 @@ bool launch(ss_server* s) {
         int64_t tiles = 0;
         while (!s->admitted.empty() &&
                static_cast<int>(slot.reqs.size()) < s->cfg.max_batch_images) {
-            const Req& q = s->admitted.front();
+            const Req q = s->admitted.front();
             if (tiles + q.tiles > s->cfg.batch_tiles) {
                 break;
             }

@@ -53,7 +53,8 @@ def test_mix_equals_alone_host_requests(persistent):
             done.extend(srv.poll(timeout_us=100_000))
         stats = srv.stats()
     assert sorted(int(c.ticket) for c in done) == sorted(tickets)
-    assert all(c.status == 0 for c in done)
+    assert all(c.status == 0 for c in done), \
+        sorted(set(int(c.status) for c in done))
     for c in done:
         assert c.submit_ns <= c.admit_ns <= c.launch_ns <= c.done_ns
     # Requests that arrived together shared batches.
