@@ -43,6 +43,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
@@ -65,6 +67,9 @@ def parse_args():
     p.add_argument("--quick", action="store_true",
                    help="skip the secondary measurements (per-image, e2e, "
                         "CPU baseline, reference GPU routes)")
+    p.add_argument("--no-extra", action="store_true",
+                   help="skip the uneven-size batch, serving and resolution "
+                        "sections")
     p.add_argument("--passes-only", action="store_true",
                    help="only run the split-pass loop (for profiling)")
     p.add_argument("--levels", type=int, default=256,
@@ -547,6 +552,12 @@ def main():
     if not args.quick:
         line.update(secondary(args, pkg, plan, images, host_images, maxs,
                               mins, stream, dist, hbm))
+        if not args.no_extra:
+            # Per-GPU measurements, run alike on every rank (no collective).
+            line["batched_uneven"] = uneven_section(args, pkg, device, stream)
+            line["served"] = serving_section(args, pkg, device, stream)
+            line["resolution_sweep"] = resolution_section(args, pkg, device,
+                                                          stream, hbm)
     elif dist.rank == 0:
         line["cpu_baseline"] = None
         line["e2e"] = None
@@ -706,6 +717,311 @@ def secondary(args, pkg, plan, images, host_images, maxs, mins, stream, dist,
         sample = [host_images[i] for i in (0, 1, 2, 3, 4)] + \
             [host_images[i] for i in range(len(images) - 5, len(images))]
         out["reference_gpu"] = reference_gpu_routes(sample, tile)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Batched uneven sizes, serving, resolution sweep
+# ---------------------------------------------------------------------------
+
+def _graph_ms(fn, stream, warmup: int, reps: int) -> float:
+    """Device ms of one call of `fn`, captured in a CUDA graph and replayed
+    back to back (CUDA events on `stream`)."""
+    import torch
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(stream):
+        fn()
+        stream.synchronize()
+        with torch.cuda.graph(g, stream=stream):
+            fn()
+    for _ in range(max(1, warmup)):
+        g.replay()
+    stream.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(reps):
+            g.replay()
+        e1.record(stream)
+    e1.synchronize()
+    del g
+    return e0.elapsed_time(e1) / reps
+
+
+def uneven_section(args, pkg, device, stream):
+    """4096 images per batch, width and height drawn independently and
+    log-uniformly from 64..1024, generators mixed 50 % smooth noise, 25 %
+    uniform-quantised (2..256 levels), 25 % plateau maps.  Plain per-image
+    launches against one batched launch (grid and persistent schedule) and the
+    autotuned per-size-class batch, all graph-replayed; every image's masks
+    are compared with its per-image result, and a sample with the oracle."""
+    import torch
+    from importlib import import_module
+    import oracle
+    synth = import_module("sparse-seam_b200.synth")
+    at = import_module("sparse-seam_b200.autotune")
+    images = synth.uneven_batch(4096, seed=20250, lo=64, hi=1024,
+                                device=device)
+    pixels = sum(im.numel() for im in images)
+    ref_max = [torch.empty_like(i) for i in images]
+    ref_min = [torch.empty_like(i) for i in images]
+    maxs = [torch.empty_like(i) for i in images]
+    mins = [torch.empty_like(i) for i in images]
+    torch.cuda.synchronize()
+    out = {"workload": ("4096 images, W and H log-uniform on 64..1024, "
+                        "mixed generators (50 % smooth noise, 25 % "
+                        "uniform-quantised, 25 % plateau maps), T=32"),
+           "images": len(images), "pixels": pixels}
+
+    big = max(images, key=lambda t: t.numel())
+    ws1 = pkg.Workspace.for_image(big.shape[1], big.shape[0], 32)
+
+    def per_image():
+        for i, im in enumerate(images):
+            pkg.extrema(im, 32, ref_max[i], ref_min[i], ws1, stream=stream)
+
+    ms = _graph_ms(per_image, stream, args.warmup, args.steps)
+    ws1.read_status(stream)
+    out["per_image"] = {"gpix_s": round(pixels / ms / 1e6, 3),
+                        "ms": round(ms, 4)}
+
+    plan = pkg.BatchPlan(images, maxs, mins, tile=32, stream=stream)
+    ws = plan.make_workspace(stream=stream)
+    for persistent in (False, True):
+        ms = _graph_ms(lambda: plan.run(ws, persistent=persistent,
+                                        stream=stream),
+                       stream, args.warmup, args.steps)
+        ws.read_status(stream)
+        key = "batched_persistent" if persistent else "batched_grid"
+        out[key] = {"gpix_s": round(pixels / ms / 1e6, 3), "ms": round(ms, 4)}
+    bad = sum(int((a != b).sum()) for a, b in
+              zip(maxs + mins, ref_max + ref_min))
+
+    import time as _time
+    t0 = _time.time()
+    table = at.tune(pixels_per_class=8 << 20, reps=3, seed=7, device=device)
+    tune_s = _time.time() - t0
+    for m in maxs + mins:
+        m.fill_(3)
+    tb = at.TunedBatch(images, maxs, mins, table, stream=stream)
+    ms = _graph_ms(lambda: tb.run(stream=stream), stream, args.warmup,
+                   args.steps)
+    tb.read_status(stream)
+    bad += sum(int((a != b).sum()) for a, b in
+               zip(maxs + mins, ref_max + ref_min))
+    out["autotuned"] = {
+        "gpix_s": round(pixels / ms / 1e6, 3), "ms": round(ms, 4),
+        "launches": len(tb.parts), "tuning_s": round(tune_s, 1),
+        "choices": {str(k): v.label() for k, v in table.choices.items()},
+        "class_bounds_px": list(at.CLASS_BOUNDS[:-1]),
+    }
+    sample = list(range(0, len(images), 64))
+    want = oracle.extrema_batch([images[i].cpu().numpy() for i in sample],
+                                threads=cpu_threads())
+    for j, i in enumerate(sample):
+        bad += int((maxs[i].cpu().numpy() != want[0][j]).sum())
+        bad += int((mins[i].cpu().numpy() != want[1][j]).sum())
+    out["mismatches"] = bad
+    out["checked"] = (f"all {len(images)} images against their per-image "
+                      f"masks, {len(sample)} against the oracle")
+    return out
+
+
+SERVE_SIZES = ((321, 481), (1024, 1024), (1356, 2040), (4096, 4096),
+               (8192, 8192))
+SERVE_WEIGHTS = (0.3, 0.3, 0.2, 0.15, 0.05)
+
+
+def _serve_images(device):
+    """Distinct host images per request size; generators from the
+    single-image, corpus and uneven-batch workloads (uniform 16 levels,
+    smooth noise, uniform-quantised, plateau maps; plateau maps only up to
+    2040x1356)."""
+    import torch
+    from importlib import import_module
+    synth = import_module("sparse-seam_b200.synth")
+    count = {0: 8, 1: 8, 2: 8, 3: 4, 4: 2}
+    pool = {}
+    for k, (h, w) in enumerate(SERVE_SIZES):
+        imgs = []
+        for j in range(count[k]):
+            kind = j % 4
+            seed = 1000 * k + j
+            if kind == 0:
+                t = synth.smooth_noise(h, w, seed, device=device).cpu()
+            elif kind == 1:
+                t = torch.from_numpy(synth.uniform_q16(h, w, seed))
+            elif kind == 2:
+                rng = np.random.default_rng(seed)
+                levels = int(rng.integers(2, 257))
+                t = torch.from_numpy(synth.quantize(
+                    rng.integers(0, 256, size=(h, w)).astype(np.uint8),
+                    levels))
+            else:
+                t = (torch.from_numpy(synth.plateau_map(h, w, seed))
+                     if h * w <= 1356 * 2040 else
+                     synth.smooth_noise(h, w, seed, device=device).cpu())
+            p = torch.empty((h, w), dtype=torch.uint8, pin_memory=True)
+            p.copy_(t)
+            imgs.append(p)
+        pool[k] = imgs
+    return pool
+
+
+def serving_section(args, pkg, device, stream):
+    """Served request stream: Poisson arrivals, each request one host image
+    whose size is drawn from 481x321 / 1024^2 / 2040x1356 / 4096^2 / 8192^2
+    (weights 0.3 / 0.3 / 0.2 / 0.15 / 0.05).  Latency = completion (masks in
+    the caller's pinned host buffers) minus scheduled arrival.  Also the
+    saturated throughput (every request at t = 0) against plain per-image
+    host-to-host calls (copy in, ss_extrema, copy out, wait) on the same
+    requests, and a mixed burst whose every result is compared with the same
+    image's result alone."""
+    import torch
+    from importlib import import_module
+    serve = import_module("sparse-seam_b200.serve")
+    pool = _serve_images(device)
+    ring = {0: 16, 1: 16, 2: 12, 3: 8, 4: 4}
+    outs = {k: [(torch.empty(SERVE_SIZES[k], dtype=torch.uint8,
+                             pin_memory=True),
+                 torch.empty(SERVE_SIZES[k], dtype=torch.uint8,
+                             pin_memory=True)) for _ in range(ring[k])]
+            for k in range(len(SERVE_SIZES))}
+    rng = np.random.default_rng(55)
+
+    def draw(n):
+        ks = rng.choice(len(SERVE_SIZES), size=n, p=SERVE_WEIGHTS)
+        return [(int(k), int(rng.integers(0, len(pool[int(k)]))))
+                for k in ks]
+
+    def maker(reqs):
+        used = {k: 0 for k in range(len(SERVE_SIZES))}
+
+        def make(i):
+            k, j = reqs[i]
+            o = outs[k][used[k] % ring[k]]
+            used[k] += 1
+            return pool[k][j], o[0], o[1]
+        return make
+
+    cfg = dict(tile=32, persistent=True, inflight=3, max_batch_images=256,
+               batch_tiles=1 << 17, pool_bytes=8 << 30)
+    out = {"workload": ("Poisson arrivals; request sizes 481x321 / 1024^2 / "
+                        "2040x1356 / 4096^2 / 8192^2 with weights "
+                        "0.3/0.3/0.2/0.15/0.05; pinned host images in, "
+                        "masks out to pinned host buffers"),
+           "server": {k: v for k, v in cfg.items()}}
+    rates = {}
+    with serve.Server(**cfg) as srv:
+        warm = draw(24)
+        serve.run_trace(srv, np.zeros(len(warm), dtype=np.int64),
+                        maker(warm))
+        for rate, dur in ((100.0, 2.0), (500.0, 2.0), (2000.0, 2.0)):
+            arrivals = serve.poisson_trace(rate, dur, seed=int(rate))
+            reqs = draw(len(arrivals))
+            res = serve.run_trace(srv, arrivals, maker(reqs))
+            d = res.as_dict()
+            d.pop("stats")
+            d["offered_gpix_s"] = round(
+                rate * float(np.dot(SERVE_WEIGHTS,
+                                    [h * w for h, w in SERVE_SIZES])) / 1e9,
+                3)
+            rates[str(int(rate))] = d
+        # Saturated: every request arrives at once.
+        sat = draw(300)
+        res = serve.run_trace(srv, np.zeros(len(sat), dtype=np.int64),
+                              maker(sat))
+        out["saturated"] = {k: v for k, v in res.as_dict().items()
+                            if k != "stats"}
+        out["server_stats"] = srv.stats()
+    out["rates_req_s"] = rates
+
+    # Plain per-image host-to-host calls on the same saturated request list.
+    big_ws = pkg.Workspace.for_image(8192, 8192, 32)
+    dev_in = torch.empty((8192, 8192), dtype=torch.uint8, device=device)
+    dev_mx = torch.empty_like(dev_in)
+    dev_mn = torch.empty_like(dev_in)
+    px = 0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for k, j in sat:
+            h, w = SERVE_SIZES[k]
+            im = pool[k][j]
+            d_in = dev_in.view(-1)[:h * w].view(h, w)
+            d_mx = dev_mx.view(-1)[:h * w].view(h, w)
+            d_mn = dev_mn.view(-1)[:h * w].view(h, w)
+            d_in.copy_(im, non_blocking=True)
+            pkg.extrema(d_in, 32, d_mx, d_mn, big_ws, stream=stream)
+            o = outs[k][0]
+            o[0].copy_(d_mx, non_blocking=True)
+            o[1].copy_(d_mn, non_blocking=True)
+            stream.synchronize()
+            px += h * w
+        e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    big_ws.read_status(stream)
+    out["per_image_h2h"] = {"gpix_s": round(px / ms / 1e6, 3),
+                            "ms": round(ms, 2), "requests": len(sat)}
+
+    # Mixed burst, distinct outputs: each result against the image alone.
+    burst = [(k, j) for k in range(len(SERVE_SIZES))
+             for j in range(min(2, len(pool[k])))] + draw(12)
+    bouts = [(torch.empty(SERVE_SIZES[k], dtype=torch.uint8, pin_memory=True),
+              torch.empty(SERVE_SIZES[k], dtype=torch.uint8, pin_memory=True))
+             for k, _ in burst]
+    with serve.Server(**cfg) as srv:
+        for i, (k, j) in enumerate(burst):
+            srv.submit(pool[k][j], *bouts[i], user=i)
+        done = []
+        while len(done) < len(burst):
+            done.extend(srv.poll(timeout_us=100_000))
+    bad = sum(1 for c in done if c.status != 0)
+    for i, (k, j) in enumerate(burst):
+        h, w = SERVE_SIZES[k]
+        d_in = pool[k][j].to(device)
+        mx, mn = pkg.extrema(d_in, 32)
+        bad += int((mx.cpu() != bouts[i][0]).sum())
+        bad += int((mn.cpu() != bouts[i][1]).sum())
+    out["mix_vs_alone_mismatches"] = bad
+    out["mix_requests"] = len(burst)
+    return out
+
+
+def resolution_section(args, pkg, device, stream, hbm):
+    """Single smooth-noise images from 1 Mpixel to 16384^2 (268 Mpixel):
+    device-resident ss_extrema, graph-replayed; each checked against the
+    oracle's row-band route."""
+    import torch
+    from importlib import import_module
+    import oracle
+    synth = import_module("sparse-seam_b200.synth")
+    out = {}
+    for side in (1024, 2048, 4096, 8192, 16384):
+        img = synth.smooth_noise(side, side, seed=side, device=device)
+        mx = torch.empty_like(img)
+        mn = torch.empty_like(img)
+        ws = pkg.Workspace.for_image(side, side, 32)
+        reps = max(3, min(args.steps, 20))
+        ms = _graph_ms(lambda: pkg.extrema(img, 32, mx, mn, ws,
+                                           stream=stream),
+                       stream, args.warmup, reps)
+        ws.read_status(stream)
+        want = oracle.extrema(img.cpu().numpy(), method="bands",
+                              threads=cpu_threads())
+        bad = int((mx.cpu().numpy() != want[0]).sum()) + \
+            int((mn.cpu().numpy() != want[1]).sum())
+        px = side * side
+        out[f"{side}x{side}"] = {
+            "us": round(ms * 1e3, 2), "gpix_s": round(px / ms / 1e6, 3),
+            "roofline_frac": round(BYTES_PER_PIXEL * px / (ms / 1e3) / 1e9
+                                   / hbm, 4),
+            "mismatches": bad}
+        del img, mx, mn, ws, want
+        torch.cuda.empty_cache()
     return out
 
 

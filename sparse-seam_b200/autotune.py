@@ -134,11 +134,18 @@ def _time_choice(images, choice: Choice, reps: int, stream):
     return e0.elapsed_time(e1) / reps, maxs, mins
 
 
+# A candidate replaces the first (the library default) only when it is at
+# least this much faster: smaller gaps are within run-to-run noise, and equal
+# choices let TunedBatch keep the classes in one launch.
+MARGIN = 0.03
+
+
 def tune(pixels_per_class: int = 16 << 20, reps: int = 5, seed: int = 0,
          device="cuda", classes: Optional[Sequence[int]] = None,
          choices: Optional[Sequence[Choice]] = None) -> TuningTable:
     """Times every candidate on a synthetic batch of each class and keeps the
-    fastest.  Raises if any candidate's masks differ from the first's."""
+    fastest (the first candidate unless another beats it by MARGIN).  Raises
+    if any candidate's masks differ from the first's."""
     import torch
     stream = torch.cuda.Stream()
     cands = list(choices) if choices else candidates()
@@ -159,7 +166,9 @@ def tune(pixels_per_class: int = 16 << 20, reps: int = 5, seed: int = 0,
                         raise RuntimeError(
                             f"class {k}: {c.label()} changed the masks")
             timings[k][c.label()] = round(ms, 4)
-            if best is None or ms < best[0]:
+            if best is None:
+                best = (ms * (1.0 - MARGIN), c)
+            elif ms < best[0]:
                 best = (ms, c)
         picked[k] = best[1]
     return TuningTable(picked, timings)
@@ -168,15 +177,25 @@ def tune(pixels_per_class: int = 16 << 20, reps: int = 5, seed: int = 0,
 class TunedBatch:
     """A batch split by size class, each part launched with its tuned choice.
 
-    Parts run one after another on one stream, so the whole batch can be
-    captured in one CUDA graph.
+    Classes whose choices differ only in the seam/resolve grouping share one
+    launch (with the grouping chosen from that launch's tile count).  Parts
+    run one after another on one stream, so the whole batch can be captured
+    in one CUDA graph.
     """
 
     def __init__(self, images: Sequence, maxima: Sequence, minima: Sequence,
                  table: TuningTable, stream=None):
         parts: Dict[Choice, List[int]] = {}
+        groups: Dict[Tuple[int, int, bool], set] = {}
+        for c in table.choices.values():
+            groups.setdefault((c.tile, c.warps, c.persistent), set()).add(
+                c.group)
         for i, im in enumerate(images):
-            parts.setdefault(table.choice_for(*im.shape), []).append(i)
+            c = table.choice_for(*im.shape)
+            key = (c.tile, c.warps, c.persistent)
+            if len(groups[key]) > 1:
+                c = Choice(c.tile, c.warps, c.persistent, 0)
+            parts.setdefault(c, []).append(i)
         self.parts: List[Tuple[Choice, object, object]] = []
         for choice, idx in sorted(parts.items(), key=lambda kv: kv[0].label()):
             plan = _pkg.BatchPlan([images[i] for i in idx],
