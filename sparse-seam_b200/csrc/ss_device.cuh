@@ -308,4 +308,28 @@ __device__ __forceinline__ void global_union(int32_t* parent, uint32_t* bits,
     err = kErrSpinLimit;
 }
 
+// Links the roots of a and b (larger below smaller) without merging flags:
+// the row-scan route ORs every fragment's flags into its root in a later
+// kernel, after all links are in place.
+__device__ __forceinline__ void global_link(int32_t* parent, int a, int b,
+                                            uint32_t& err) {
+#pragma unroll 1
+    for (int it = 0; it < kGlobalBound; ++it) {
+        a = global_find(parent, a, err);
+        b = global_find(parent, b, err);
+        if (a == b || err) {
+            return;
+        }
+        const int hi = a > b ? a : b;
+        const int lo = a > b ? b : a;
+        const int old = atomicCAS(parent + hi, hi, lo);
+        if (old == hi) {
+            return;
+        }
+        a = old;
+        b = lo;
+    }
+    err = kErrSpinLimit;
+}
+
 }  // namespace ss

@@ -39,6 +39,7 @@
 #include "sparse_seam.h"
 #include "ss_internal.h"
 #include "ss_rowscan.cuh"
+#include "ss_runs.cuh"
 #include "ss_tile.cuh"
 
 namespace ss {
@@ -469,6 +470,44 @@ rowscan_tile_pass_kernel(Source src, Arena a) {
     }
 }
 
+// Run-mask variant of the tile pass (same contract, same later passes).
+template <int NW, bool kPersistent>
+__global__ void __launch_bounds__(NW * 32)
+runs_tile_pass_kernel(Source src, Arena a) {
+    __shared__ rowscan::RunSmem sm[NW];
+    const int warp = static_cast<int>(threadIdx.x) >> 5;
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    if (a.header->magic != kMagic) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            raise_error(a.header, kErrUninitialized, 0u);
+        }
+        return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.header->last_tiles = static_cast<uint64_t>(src.total_tiles);
+        a.header->tile = rowscan::T;
+    }
+    if constexpr (kPersistent) {
+        for (;;) {
+            uint32_t item = 0;
+            if (lane == 0) {
+                item = atomicAdd(&a.header->queue_head, 1u);
+            }
+            item = __shfl_sync(~0u, item, 0);
+            if (static_cast<int64_t>(item) >= src.total_tiles) {
+                break;
+            }
+            rowscan::tile_pass_runs_warp(sm[warp], src, a, item);
+            __syncwarp();
+        }
+    } else {
+        const int64_t item = static_cast<int64_t>(blockIdx.x) * NW + warp;
+        if (item < src.total_tiles) {
+            rowscan::tile_pass_runs_warp(sm[warp], src, a, item);
+        }
+    }
+}
+
 // Seam and resolve passes: each warp takes src.group consecutive tiles.
 template <int NW, bool kPersistent>
 __global__ void __launch_bounds__(NW * 32)
@@ -482,6 +521,20 @@ rowscan_seam_pass_kernel(Source src, Arena a) {
         (static_cast<int64_t>(blockIdx.x) * NW + warp) * src.group;
     if (first < src.total_tiles) {
         rowscan::seam_pass_warp32(src, a, first);
+    }
+}
+
+template <int NW>
+__global__ void __launch_bounds__(NW * 32)
+rowscan_flags_pass_kernel(Source src, Arena a) {
+    if (a.header->magic != kMagic) {
+        return;
+    }
+    const int warp = static_cast<int>(threadIdx.x) >> 5;
+    const int64_t first =
+        (static_cast<int64_t>(blockIdx.x) * NW + warp) * src.group;
+    if (first < src.total_tiles) {
+        rowscan::flags_pass_warp32(src, a, first);
     }
 }
 
@@ -642,13 +695,14 @@ struct Config {
     int items_per_cta;   // tiles one tile-pass CTA handles per launch slot
     Kernel seam_pass;    // between the two passes, or nullptr
     int later_per_cta;   // tiles one seam / resolve CTA handles
+    Kernel flags_pass;   // after the seam pass, or nullptr
 };
 
 #define SS_CONFIG(T, NW)                                                      \
     Config {                                                                  \
         T, NW, {tile_pass_kernel<T, NW, false>, tile_pass_kernel<T, NW, true>}, \
             {resolve_pass_kernel<T, NW, false>,                               \
-             resolve_pass_kernel<T, NW, true>}, 1, nullptr, 1                 \
+             resolve_pass_kernel<T, NW, true>}, 1, nullptr, 1, nullptr        \
     }
 // Row-scan configurations are listed with warps = -NW (one tile per warp).
 #define SS_ROWSCAN(NW)                                                        \
@@ -658,17 +712,31 @@ struct Config {
              rowscan_tile_pass_kernel<NW, true>},                             \
             {rowscan_resolve_pass_kernel<NW, false>,                          \
              rowscan_resolve_pass_kernel<NW, true>}, NW,                      \
-            rowscan_seam_pass_kernel<NW, false>, 32 * NW                      \
+            rowscan_seam_pass_kernel<NW, false>, 32 * NW,                     \
+            rowscan_flags_pass_kernel<NW>                                     \
+    }
+
+// Run-mask row-scan configurations are listed with warps = -(16 + NW).
+#define SS_RUNS(NW)                                                           \
+    Config {                                                                  \
+        32, -(16 + (NW)),                                                     \
+            {runs_tile_pass_kernel<NW, false>,                                \
+             runs_tile_pass_kernel<NW, true>},                                \
+            {rowscan_resolve_pass_kernel<NW, false>,                          \
+             rowscan_resolve_pass_kernel<NW, true>}, NW,                      \
+            rowscan_seam_pass_kernel<NW, false>, 32 * NW,                     \
+            rowscan_flags_pass_kernel<NW>                                     \
     }
 
 static const Config kConfigs[] = {
     SS_CONFIG(16, 2), SS_CONFIG(16, 4), SS_CONFIG(16, 8),
     SS_CONFIG(32, 4), SS_CONFIG(32, 8), SS_CONFIG(32, 16),
     SS_CONFIG(64, 8), SS_CONFIG(64, 16),
-    SS_ROWSCAN(2), SS_ROWSCAN(4),
+    SS_ROWSCAN(2), SS_ROWSCAN(4), SS_RUNS(2), SS_RUNS(4),
 };
 #undef SS_CONFIG
 #undef SS_ROWSCAN
+#undef SS_RUNS
 
 // Per tile size, the configuration used by default (index by tile / 16 - 1);
 // negative warps select the row-scan kernels.
@@ -771,7 +839,7 @@ static ss_status launch_route(const Config& cfg, const Source& src_in,
     // the launches below.
     (void)cudaGetLastError();
     Source src = src_in;
-    const int nw = cfg.warps < 0 ? -cfg.warps : cfg.warps;
+    const int nw = cfg.warps < 0 ? (-cfg.warps) % 16 : cfg.warps;
     const int threads = nw * 32;
     // Tiles per CTA of the passes after the tile pass.
     int later_per_cta = cfg.later_per_cta;
@@ -802,6 +870,10 @@ static ss_status launch_route(const Config& cfg, const Source& src_in,
     if ((passes & 4) && cfg.seam_pass) {
         cfg.seam_pass<<<static_cast<unsigned>(ctas2), threads, 0, stream>>>(
             src, arena);
+        if (cfg.flags_pass) {
+            cfg.flags_pass<<<static_cast<unsigned>(ctas2), threads, 0,
+                             stream>>>(src, arena);
+        }
     }
     if (passes & 2) {
         cfg.resolve_pass[p]<<<grid2, threads, 0, stream>>>(src, arena);

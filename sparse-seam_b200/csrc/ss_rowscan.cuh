@@ -56,6 +56,9 @@ constexpr int kHaloW = T + 2;          // staged row: columns x0-1 .. x0+T
 constexpr int kSeamCap = 12 * T;       // seam items per tile
 constexpr uint32_t kDeadRecord = 0xFEu;  // border record of a decided zone
 constexpr uint32_t kNoRecord = 0xFFu;    // border pixel of an inside zone
+// Resolve pass: tiles with at most this many logged runs are written run by
+// run; denser tiles row by row.
+constexpr uint32_t kSparseRuns = 16u;
 
 // Per-pixel shared word: bits 0-9 parent, 10-12 zone flags (at roots),
 // 13-20 record + 1 (at roots of live seam zones), 21-23 own flags.
@@ -647,6 +650,10 @@ __device__ __forceinline__ void seam_pass_warp32(const Source& src,
         const int64_t g = first + owner;
         const int64_t tx = __shfl_sync(~0u, tiles_x, owner);
         const uint32_t j = f - __shfl_sync(~0u, excl, owner);
+        // What the item asks for: unite fragment fo with fragment `target`,
+        // or (target == -1) OR "both flags" into fo.
+        int fo = -1;
+        int target = -2;
         if (f < total) {
             const uint32_t it = __ldcg(a.seam_items + g * kSeamCap + j);
             const uint32_t rec = it & 0xFFu;
@@ -656,23 +663,83 @@ __device__ __forceinline__ void seam_pass_warp32(const Source& src,
             if (rec >= static_cast<uint32_t>(kSlots) || ng < 0 ||
                 ng >= src.total_tiles) {
                 err = kErrRecordRange;
-                continue;
-            }
-            const uint32_t rn = __ldg(a.border + ng * kSlots + off);
-            const int fo = static_cast<int>(g * kSlots + rec);
-            if (rn == kDeadRecord) {
-                global_or(a.parent, a.bits, fo, kDead, err);
-            } else if (rn < static_cast<uint32_t>(kSlots)) {
-                global_union(a.parent, a.bits, fo,
-                             static_cast<int>(ng * kSlots + rn), err);
             } else {
-                err = kErrInvariant;   // equal across a seam, no seam zone
+                const uint32_t rn = __ldg(a.border + ng * kSlots + off);
+                if (rn == kDeadRecord) {
+                    fo = static_cast<int>(g * kSlots + rec);
+                    target = -1;
+                } else if (rn < static_cast<uint32_t>(kSlots)) {
+                    fo = static_cast<int>(g * kSlots + rec);
+                    target = static_cast<int>(ng * kSlots + rn);
+                } else {
+                    err = kErrInvariant;   // equal across a seam, no seam zone
+                }
+            }
+        }
+        // Neighbouring border pixels of one zone pair repeat the same request
+        // (items are stored in border order): only the first of a streak
+        // acts.
+        const int prev_fo = __shfl_up_sync(~0u, fo, 1);
+        const int prev_target = __shfl_up_sync(~0u, target, 1);
+        const bool repeat = lane > 0 && prev_fo == fo && prev_target == target;
+        if (fo >= 0 && !repeat) {
+            if (target == -1) {
+                // The fragment's own word; the flags pass carries it to the
+                // component's root.
+                atomicOr(a.bits + fo, kDead);
+            } else {
+                global_link(a.parent, fo, target, err);
             }
         }
     }
     if (err) {
         raise_error(a.header, err, static_cast<uint32_t>(first));
     }
+}
+
+// Flags pass (after the seam pass, before the resolve pass): every live
+// fragment ORs its flags (its zone's flags and the "decided neighbour across
+// a seam" marks of the seam pass) into its component's root.  The kernel
+// boundaries order it after every link and before every read of a root.
+__device__ __forceinline__ void flags_pass_warp32(const Source& src,
+                                                  const Arena& a,
+                                                  int64_t first) {
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    const int64_t tile = first + lane;
+    const bool valid = lane < src.group && tile < src.total_tiles;
+    const uint32_t k =
+        valid ? min(static_cast<uint32_t>(a.fragment_count[tile]),
+                    static_cast<uint32_t>(kSlots))
+              : 0u;
+    uint32_t total = 0;
+    const uint32_t excl = warp_prefix(k, total);
+    uint32_t err = 0;
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t f = base + static_cast<uint32_t>(lane);
+        const int owner = owner_of(excl, f);
+        const uint32_t r = f - __shfl_sync(~0u, excl, owner);
+        if (f < total) {
+            const int fr = static_cast<int>((first + owner) * kSlots + r);
+            const int root = global_find(a.parent, fr, err);
+            if (root != fr) {
+                const uint32_t own = ld_relaxed(a.bits + fr) & 3u;
+                if (own && (ld_relaxed(a.bits + root) & own) != own) {
+                    atomicOr(a.bits + root, own);
+                }
+            }
+        }
+    }
+    if (err) {
+        raise_error(a.header, err, static_cast<uint32_t>(first));
+    }
+}
+
+// Bytes 0x00 / 0xFF of the low 4 bits of `bits` (bit i -> byte i): the
+// product adds copies of the 4 bits shifted by 0, 7, 14 and 21, which puts
+// bit i at bit 8i (the copies do not overlap, so nothing carries); the mask
+// keeps bits 0, 8, 16 and 24, and the multiply by 0xFF fills each byte.
+__device__ __forceinline__ uint32_t spread4(uint32_t bits) {
+    return (((bits & 15u) * 0x00204081u) & 0x01010101u) * 0xFFu;
 }
 
 struct __align__(16) ResolveSmem {
@@ -683,7 +750,68 @@ struct __align__(16) ResolveSmem {
     int32_t out_pitch[32];
     int16_t tw[32];
     int16_t th[32];
+    uint32_t live[T];         // one tile at a time: logged pixels per row,
+    uint32_t vmax[T];         //   and those whose maxima / minima byte is 255
+    uint32_t vmin[T];
 };
+
+// Rewrites the logged pixels of a full tile (32 x 32, rows and origins
+// aligned to `vec` = 16, 8 or 4 bytes) from per-row bit masks: each lane
+// takes one `vec`-byte piece of a row (32 / vec lanes per row, vec rows per
+// step), loads it unless every byte is logged, replaces the logged bytes and
+// stores it back.
+__device__ __forceinline__ uint32_t merge4(uint32_t cur, uint32_t live,
+                                          uint32_t verdict) {
+    const uint32_t m = spread4(live);
+    return (cur & ~m) | (spread4(verdict) & m);
+}
+
+__device__ __forceinline__ void merge_rows(uint8_t* omax, uint8_t* omin,
+                                           int64_t pitch,
+                                           const uint32_t* live,
+                                           const uint32_t* vmax,
+                                           const uint32_t* vmin, int vec) {
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    const int per_row = T / vec;
+    const int c = lane % per_row;
+    const int rr = lane / per_row;
+    const uint32_t full = (vec == 16) ? 0xFFFFu : (vec == 8) ? 0xFFu : 0xFu;
+    for (int r0 = 0; r0 < T; r0 += vec) {
+        const int r = r0 + rr;
+        const uint32_t lv = (live[r] >> (c * vec)) & full;
+        if (lv == 0u) {
+            continue;
+        }
+        const uint32_t bx = vmax[r] >> (c * vec);
+        const uint32_t bn = vmin[r] >> (c * vec);
+        const int64_t o = static_cast<int64_t>(r) * pitch + c * vec;
+        const bool all = lv == full;
+        if (vec == 16) {
+            uint4* px = reinterpret_cast<uint4*>(omax + o);
+            uint4* pn = reinterpret_cast<uint4*>(omin + o);
+            const uint4 cx = all ? make_uint4(0u, 0u, 0u, 0u) : *px;
+            const uint4 cn = all ? make_uint4(0u, 0u, 0u, 0u) : *pn;
+            *px = make_uint4(merge4(cx.x, lv, bx), merge4(cx.y, lv >> 4, bx >> 4),
+                             merge4(cx.z, lv >> 8, bx >> 8),
+                             merge4(cx.w, lv >> 12, bx >> 12));
+            *pn = make_uint4(merge4(cn.x, lv, bn), merge4(cn.y, lv >> 4, bn >> 4),
+                             merge4(cn.z, lv >> 8, bn >> 8),
+                             merge4(cn.w, lv >> 12, bn >> 12));
+        } else if (vec == 8) {
+            uint2* px = reinterpret_cast<uint2*>(omax + o);
+            uint2* pn = reinterpret_cast<uint2*>(omin + o);
+            const uint2 cx = all ? make_uint2(0u, 0u) : *px;
+            const uint2 cn = all ? make_uint2(0u, 0u) : *pn;
+            *px = make_uint2(merge4(cx.x, lv, bx), merge4(cx.y, lv >> 4, bx >> 4));
+            *pn = make_uint2(merge4(cn.x, lv, bn), merge4(cn.y, lv >> 4, bn >> 4));
+        } else {
+            uint32_t* px = reinterpret_cast<uint32_t*>(omax + o);
+            uint32_t* pn = reinterpret_cast<uint32_t*>(omin + o);
+            *px = merge4(all ? 0u : *px, lv, bx);
+            *pn = merge4(all ? 0u : *pn, lv, bn);
+        }
+    }
+}
 
 __device__ __forceinline__ void resolve_warp32(ResolveSmem& sm,
                                                const Source& src,
@@ -735,36 +863,114 @@ __device__ __forceinline__ void resolve_warp32(ResolveSmem& sm,
     }
     flipped = __reduce_or_sync(~0u, flipped);
     __syncwarp();
-    // The logged runs.
-    for (uint32_t base = 0; base < total_n; base += 32) {
+    // Tiles with few logged runs: all of the group's runs together, their
+    // bytes spread over the lanes (consecutive lanes write consecutive bytes
+    // of a run).
+    const uint32_t n_sparse = n <= kSparseRuns ? n : 0u;
+    uint32_t total_sparse = 0u;
+    const uint32_t excl_s = warp_prefix(n_sparse, total_sparse);
+    for (uint32_t base = 0; base < total_sparse; base += 32) {
         const uint32_t e = base + static_cast<uint32_t>(lane);
-        const int owner = owner_of(excl_n, e);
-        const uint32_t j = e - __shfl_sync(~0u, excl_n, owner);
+        const int owner = owner_of(excl_s, e);
+        const uint32_t j = e - __shfl_sync(~0u, excl_s, owner);
         const uint32_t kown = __shfl_sync(~0u, k, owner);
-        if (e < total_n) {
+        uint32_t len = 0u;
+        int64_t off = 0;
+        uint32_t verdict = 0u;
+        if (e < total_sparse) {
             const uint32_t ent =
                 __ldcg(a.pending + (first + owner) * kPendingCap + j);
             const uint32_t rec = ent & 0xFFu;
             const int x = static_cast<int>((ent >> 8) & 63u);
             const int y = static_cast<int>((ent >> 14) & 63u);
-            const int len = static_cast<int>((ent >> 20) & 127u);
-            if (rec >= kown ||
-                x + len > sm.tw[owner] || y >= sm.th[owner] || len == 0) {
+            const int n_px = static_cast<int>((ent >> 20) & 127u);
+            if (rec >= kown || x + n_px > sm.tw[owner] || y >= sm.th[owner] ||
+                n_px == 0) {
+                err = kErrRecordRange;
+            } else {
+                const uint32_t fl = sm.final_flags[owner][rec];
+                verdict = ((fl & kHasGreater) ? 0u : 0xFFu) |
+                          ((fl & kHasSmaller) ? 0u : 0xFF00u);
+                off = sm.out_origin[owner] +
+                      static_cast<int64_t>(y) * sm.out_pitch[owner] + x;
+                len = static_cast<uint32_t>(n_px);
+            }
+        }
+        uint32_t bytes = 0u;
+        const uint32_t excl_len = warp_prefix(len, bytes);
+        for (uint32_t b0 = 0; b0 < bytes; b0 += 32) {
+            const uint32_t bi = b0 + static_cast<uint32_t>(lane);
+            const int src_lane = owner_of(excl_len, bi);
+            const int tile_of = __shfl_sync(~0u, owner, src_lane);
+            const int64_t o = __shfl_sync(~0u, off, src_lane) +
+                              (bi - __shfl_sync(~0u, excl_len, src_lane));
+            const uint32_t vd = __shfl_sync(~0u, verdict, src_lane);
+            if (bi < bytes) {
+                sm.maxima[tile_of][o] = static_cast<uint8_t>(vd);
+                sm.minima[tile_of][o] = static_cast<uint8_t>(vd >> 8);
+            }
+        }
+    }
+    // Tiles with many logged runs, one at a time: their pixels and verdicts
+    // as row masks, then the tile's rows rewritten (logged bytes replaced,
+    // the others kept).
+    for (int t = 0; t < src.group; ++t) {
+        const uint32_t nt = __shfl_sync(~0u, n, t);
+        if (nt <= kSparseRuns) {
+            continue;
+        }
+        const uint32_t kt = __shfl_sync(~0u, k, t);
+        sm.live[lane] = 0u;
+        sm.vmax[lane] = 0u;
+        sm.vmin[lane] = 0u;
+        __syncwarp();
+        const int tw = sm.tw[t];
+        const int th = sm.th[t];
+        const uint32_t* plog = a.pending + (first + t) * kPendingCap;
+        for (uint32_t e = static_cast<uint32_t>(lane); e < nt; e += 32u) {
+            const uint32_t ent = __ldcg(plog + e);
+            const uint32_t rec = ent & 0xFFu;
+            const int x = static_cast<int>((ent >> 8) & 63u);
+            const int y = static_cast<int>((ent >> 14) & 63u);
+            const int n_px = static_cast<int>((ent >> 20) & 127u);
+            if (rec >= kt || x + n_px > tw || y >= th || n_px == 0) {
                 err = kErrRecordRange;
                 continue;
             }
-            const uint32_t fl = sm.final_flags[owner][rec];
-            const uint8_t mx = (fl & kHasGreater) ? 0 : 255;
-            const uint8_t mn = (fl & kHasSmaller) ? 0 : 255;
-            const int64_t o = sm.out_origin[owner] +
-                              static_cast<int64_t>(y) * sm.out_pitch[owner] + x;
-            uint8_t* pmx = sm.maxima[owner] + o;
-            uint8_t* pmn = sm.minima[owner] + o;
-            for (int q = 0; q < len; ++q) {
-                pmx[q] = mx;
-                pmn[q] = mn;
+            const uint32_t fl = sm.final_flags[t][rec];
+            const uint32_t R = ((2u << (x + n_px - 1)) - 1u) & ~((1u << x) - 1u);
+            atomicOr(&sm.live[y], R);
+            if (!(fl & kHasGreater)) {
+                atomicOr(&sm.vmax[y], R);
+            }
+            if (!(fl & kHasSmaller)) {
+                atomicOr(&sm.vmin[y], R);
             }
         }
+        __syncwarp();
+        uint8_t* omax = sm.maxima[t] + sm.out_origin[t];
+        uint8_t* omin = sm.minima[t] + sm.out_origin[t];
+        const int64_t pitch = sm.out_pitch[t];
+        const uint64_t align = reinterpret_cast<uint64_t>(omax) |
+                               reinterpret_cast<uint64_t>(omin) |
+                               static_cast<uint64_t>(pitch);
+        int vec = (align & 15u) == 0 ? 16 : (align & 7u) == 0 ? 8
+                : (align & 3u) == 0 ? 4 : 1;
+        if (tw < T || th < T) {
+            vec = 1;
+        }
+        if (vec > 1) {
+            merge_rows(omax, omin, pitch, sm.live, sm.vmax, sm.vmin, vec);
+        } else {
+            for (int r = 0; r < th; ++r) {
+                if ((sm.live[r] >> lane) & 1u) {
+                    const int64_t o = static_cast<int64_t>(r) * pitch + lane;
+                    omax[o] = ((sm.vmax[r] >> lane) & 1u) ? 255 : 0;
+                    omin[o] = ((sm.vmin[r] >> lane) & 1u) ? 255 : 0;
+                }
+            }
+        }
+        __syncwarp();
     }
     if (lane == 0 && flipped) {
         atomicAdd(&a.header->flipped_tiles, __popc(flipped));

@@ -1,0 +1,637 @@
+// ss_runs.cuh -- T = 32 tile pass on per-row bit masks and runs.
+//
+// Same contract as tile_pass_warp (ss_rowscan.cuh): one warp per 32 x 32
+// tile; the pixels other than "decided" ones (with both a greater and a
+// smaller 8-neighbour) are labelled into flat zones, live seam zones are
+// numbered and logged for the seam and resolve passes, and every pixel
+// outside a live zone gets its mask bytes in one final row pass (whole
+// 32-byte rows where the row holds no live pixel).  The difference is the representation of the
+// listed pixels: instead of a per-pixel list, the row scan leaves seven
+// 32-bit masks per tile row in the registers of lane y = row:
+//   L    listed pixels
+//   GT   listed pixels with a strictly greater 8-neighbour
+//   LT   listed pixels with a strictly smaller 8-neighbour
+//   EU   pixels equal to the pixel above          (bit x: v(x,y) == v(x,y-1))
+//   EUL  pixels equal to the pixel above-left     (v(x,y) == v(x-1,y-1))
+//   EUR  pixels equal to the pixel above-right    (v(x,y) == v(x+1,y-1))
+//   EL   pixels equal to the pixel on the left    (v(x,y) == v(x-1,y))
+// From these, with shifts and the neighbouring rows' masks (shuffles):
+//   runs      maximal horizontal runs of equal listed pixels (heads, ends);
+//   dead      listed pixels with an equal decided neighbour in the tile
+//             (their zone holds a decided pixel, so it is in no mask);
+//   seam      listed pixels with an equal neighbour outside the tile;
+//   links     one union per pair of 8-adjacent equal runs in consecutive
+//             rows, at the first column of their contact (three cases, as in
+//             tile_pass_warp's phase C).
+// Union-find runs over run heads only, one lane per row, so its cost grows
+// with the number of runs and contacts per row rather than with the number
+// of listed pixels: large plateaus cost a few runs per row.
+//
+// Reference behaviour followed (paths inside the reference repository):
+// zone flags and seam test, harness/primary/snapshot_sparse_seam_cuda_v1_0.cu
+// :340-390; per-tile fragment records, :392-410; cross-seam merge of equal
+// 8-adjacent border pixels, :508-581; masks from the resolved flags, :477-506.
+#pragma once
+
+#include "ss_rowscan.cuh"
+
+namespace ss {
+
+namespace rowscan {
+
+struct __align__(16) RunSmem {
+    uint32_t word[T * T];          // union-find word at each run head
+    int16_t img[kHaloW * kHaloW];  // tile + halo, -1 outside the image
+};
+
+// Run-head words use the layout of the list kernels (bits 10-12 zone flags,
+// 13-20 record + 1) but store the parent as (parent XOR self) in bits 0-9,
+// so an all-zero word is a root with no flags: the words start zeroed.
+__device__ __forceinline__ int rparent(uint32_t w, int x) {
+    return static_cast<int>((w & kParMask) ^ static_cast<uint32_t>(x));
+}
+
+__device__ __forceinline__ uint32_t with_parent(uint32_t w, int x, int p) {
+    return (w & ~kParMask) | static_cast<uint32_t>(p ^ x);
+}
+
+// Find with path halving (used while linking: a non-root word changes only
+// in its parent bits, and halving writes an ancestor).
+__device__ __forceinline__ int rfind(volatile uint32_t* w, int x,
+                                     uint32_t& err) {
+#pragma unroll 1
+    for (int it = 0; it < T * T; ++it) {
+        const uint32_t wx = w[x];
+        const int p = rparent(wx, x);
+        if (p == x) {
+            return x;
+        }
+        const int gp = rparent(w[p], p);
+        if (gp == p) {
+            return p;
+        }
+        w[x] = with_parent(wx, x, gp);
+        x = gp;
+    }
+    err = kErrSpinLimit;
+    return x;
+}
+
+// Links the larger root below the smaller one (CAS on the whole word).
+__device__ __forceinline__ void runion(uint32_t* w_, int a, int b,
+                                       uint32_t& err) {
+    volatile uint32_t* w = w_;
+#pragma unroll 1
+    for (int it = 0; it < 4 * T * T; ++it) {
+        a = rfind(w, a, err);
+        b = rfind(w, b, err);
+        if (a == b || err) {
+            return;
+        }
+        const int hi = a > b ? a : b;
+        const int lo = a > b ? b : a;
+        const uint32_t cur = w[hi];
+        if (rparent(cur, hi) != hi) {
+            continue;
+        }
+        if (atomicCAS(w_ + hi, cur, with_parent(cur, hi, lo)) == cur) {
+            return;
+        }
+    }
+    err = kErrSpinLimit;
+}
+
+// Word of the run whose head is column h of row y.  The column is XORed with
+// the row so that the lanes of a lane-per-row step, which often touch heads
+// in the same column, hit 32 different shared-memory banks; within a row
+// the map is a permutation, so every (y, h) keeps its own word.
+__device__ __forceinline__ int run_word(int y, int h) {
+    return (y << 5) | (h ^ y);
+}
+
+// Head of the run holding bit x of a row whose run heads are `heads`.
+__device__ __forceinline__ int head_of(uint32_t heads, int x) {
+    return 31 - __clz(heads & le_mask_of(x));
+}
+
+// Bits lo..hi (0 <= lo <= hi <= 31).
+__device__ __forceinline__ uint32_t range_mask(int lo, int hi) {
+    return ((2u << hi) - 1u) & ~((1u << lo) - 1u);
+}
+
+// Writes the 32 x 32 mask bytes of a full tile from per-row bit masks held
+// by lane = row (`mxb`, `mnb`: 1 = byte 255), `vec` bytes per store (16, 8
+// or 4; rows and bases aligned to it).  Each store instruction covers
+// 32 * vec bytes: 32 / vec lanes per row, vec rows per instruction.
+__device__ __forceinline__ void store_rows(uint8_t* omax, uint8_t* omin,
+                                           const TileGeom& g,
+                                           int64_t out_pitch, uint32_t mxb,
+                                           uint32_t mnb, int vec) {
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    const int per_row = T / vec;
+    const int c = lane % per_row;
+    const int rr = lane / per_row;
+    for (int r0 = 0; r0 < T; r0 += vec) {
+        const int r = r0 + rr;
+        const uint32_t bx = __shfl_sync(~0u, mxb, r) >> (c * vec);
+        const uint32_t bn = __shfl_sync(~0u, mnb, r) >> (c * vec);
+        const int64_t o =
+            static_cast<int64_t>(g.y0 + r) * out_pitch + g.x0 + c * vec;
+        if (vec == 16) {
+            *reinterpret_cast<uint4*>(omax + o) =
+                make_uint4(spread4(bx), spread4(bx >> 4), spread4(bx >> 8),
+                           spread4(bx >> 12));
+            *reinterpret_cast<uint4*>(omin + o) =
+                make_uint4(spread4(bn), spread4(bn >> 4), spread4(bn >> 8),
+                           spread4(bn >> 12));
+        } else if (vec == 8) {
+            *reinterpret_cast<uint2*>(omax + o) =
+                make_uint2(spread4(bx), spread4(bx >> 4));
+            *reinterpret_cast<uint2*>(omin + o) =
+                make_uint2(spread4(bn), spread4(bn >> 4));
+        } else {
+            *reinterpret_cast<uint32_t*>(omax + o) = spread4(bx);
+            *reinterpret_cast<uint32_t*>(omin + o) = spread4(bn);
+        }
+    }
+}
+
+__device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
+                                                    const Source& src,
+                                                    const Arena& a,
+                                                    int64_t item) {
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint32_t le_mask = lt_mask | (1u << lane);
+    uint32_t err = 0;
+
+    const PlanImage job = load_job(src, item);
+    const TileGeom g = tile_geom(job, item - job.tile_base);
+    const uint8_t* __restrict__ img = job.image;
+    const int64_t pitch = job.pitch;
+    const int width = job.width;
+    const int height = job.height;
+    const int64_t out_pitch = job.out_pitch;
+    uint8_t* __restrict__ omax = job.maxima;
+    uint8_t* __restrict__ omin = job.minima;
+
+    // -- prologue: stage the tile and its halo; zero the words --------------
+    // Staged row r holds image row y0 - 1 + r, staged column c image column
+    // x0 - 1 + c.
+    {
+        const int gx = g.x0 + lane;
+        const bool col_ok = lane < g.tw;
+        int vals[T + 2];
+#pragma unroll
+        for (int r = 0; r < T + 2; ++r) {
+            const int gy = g.y0 + r - 1;
+            vals[r] = (col_ok && static_cast<unsigned>(gy) <
+                                     static_cast<unsigned>(height))
+                          ? static_cast<int>(__ldg(img + gy * pitch + gx))
+                          : -1;
+        }
+        const int xl = g.x0 - 1;
+        const int xr = g.x0 + T;
+        const int gy0 = g.y0 - 1 + lane;
+        const int gy1 = g.y0 + 31 + lane;
+        const bool ok0 =
+            static_cast<unsigned>(gy0) < static_cast<unsigned>(height);
+        const bool ok1 = lane < 2 && static_cast<unsigned>(gy1) <
+                                         static_cast<unsigned>(height);
+        const int hl0 = (xl >= 0 && ok0)
+                            ? static_cast<int>(__ldg(img + gy0 * pitch + xl))
+                            : -1;
+        const int hr0 = (xr < width && ok0)
+                            ? static_cast<int>(__ldg(img + gy0 * pitch + xr))
+                            : -1;
+        const int hl1 = (xl >= 0 && ok1)
+                            ? static_cast<int>(__ldg(img + gy1 * pitch + xl))
+                            : -1;
+        const int hr1 = (xr < width && ok1)
+                            ? static_cast<int>(__ldg(img + gy1 * pitch + xr))
+                            : -1;
+#pragma unroll
+        for (int r = 0; r < T + 2; ++r) {
+            sm.img[r * kHaloW + lane + 1] = static_cast<int16_t>(vals[r]);
+        }
+        sm.img[lane * kHaloW] = static_cast<int16_t>(hl0);
+        sm.img[lane * kHaloW + kHaloW - 1] = static_cast<int16_t>(hr0);
+        if (lane < 2) {
+            sm.img[(32 + lane) * kHaloW] = static_cast<int16_t>(hl1);
+            sm.img[(32 + lane) * kHaloW + kHaloW - 1] =
+                static_cast<int16_t>(hr1);
+        }
+        uint4* w4 = reinterpret_cast<uint4*>(sm.word);
+#pragma unroll
+        for (int k = 0; k < T * T / 128; ++k) {
+            w4[k * 32 + lane] = make_uint4(0u, 0u, 0u, 0u);
+        }
+    }
+    __syncwarp();
+
+    // -- row scan: flags, decided pixels, row masks ----------------------------
+    const bool col_ok = lane < g.tw;
+    uint32_t rL = 0, rGT = 0, rLT = 0, rEU = 0, rEUL = 0, rEUR = 0, rEL = 0;
+    {
+        const int16_t* scol = sm.img + lane;   // staged columns lane .. lane + 2
+        int Lp = scol[0];
+        int vp = scol[1];
+        int Rp = scol[2];
+        int Lc = scol[kHaloW];
+        int vc = scol[kHaloW + 1];
+        int Rc = scol[kHaloW + 2];
+        int hmax_p = max(max(Lp, vp), Rp);
+        unsigned hmin_p = min(min(static_cast<unsigned>(Lp),
+                                  static_cast<unsigned>(vp)),
+                              static_cast<unsigned>(Rp));
+        int hmax_c = max(max(Lc, vc), Rc);
+        unsigned hmin_c = min(min(static_cast<unsigned>(Lc),
+                                  static_cast<unsigned>(vc)),
+                              static_cast<unsigned>(Rc));
+#pragma unroll 2
+        for (int y = 0; y < g.th; ++y) {
+            const int16_t* nrow = scol + (y + 2) * kHaloW;
+            const int Ln = nrow[0];
+            const int vn = nrow[1];
+            const int Rn = nrow[2];
+            const int hmax_n = max(max(Ln, vn), Rn);
+            const unsigned hmin_n =
+                min(min(static_cast<unsigned>(Ln), static_cast<unsigned>(vn)),
+                    static_cast<unsigned>(Rn));
+            const int mx = max(max(hmax_p, hmax_n), max(Lc, Rc));
+            const unsigned mn = min(min(hmin_p, hmin_n),
+                                    min(static_cast<unsigned>(Lc),
+                                        static_cast<unsigned>(Rc)));
+            const bool gt = mx > vc;
+            const bool lt = mn < static_cast<unsigned>(vc);
+            const bool listed = col_ok && !(gt && lt);
+            const uint32_t bL = __ballot_sync(~0u, listed);
+            const uint32_t bGT = __ballot_sync(~0u, listed && gt);
+            const uint32_t bLT = __ballot_sync(~0u, listed && lt);
+            const uint32_t bEU = __ballot_sync(~0u, col_ok && vc == vp);
+            const uint32_t bEUL = __ballot_sync(~0u, col_ok && vc == Lp);
+            const uint32_t bEUR = __ballot_sync(~0u, col_ok && vc == Rp);
+            const uint32_t bEL = __ballot_sync(~0u, col_ok && vc == Lc);
+            if (lane == y) {
+                rL = bL;
+                rGT = bGT;
+                rLT = bLT;
+                rEU = bEU;
+                rEUL = bEUL;
+                rEUR = bEUR;
+                rEL = bEL;
+            }
+            hmax_p = hmax_c;
+            hmin_p = hmin_c;
+            hmax_c = hmax_n;
+            hmin_c = hmin_n;
+            Lp = Lc;
+            vp = vc;
+            Rp = Rc;
+            vc = vn;
+            Lc = Ln;
+            Rc = Rn;
+        }
+    }
+
+    // Staged pixel (x, y) of the tile, x and y in -1 .. T.
+    auto px = [&](int x, int y) -> int {
+        return sm.img[(y + 1) * kHaloW + x + 1];
+    };
+
+    // -- seam masks: border pixels with an equal neighbour outside the tile --
+    uint32_t sT, sB, sLc, sRc;
+    {
+        const int x = lane;
+        const int v0 = px(x, 0);
+        sT = __ballot_sync(~0u, x < g.tw && (px(x - 1, -1) == v0 ||
+                                             px(x, -1) == v0 ||
+                                             px(x + 1, -1) == v0));
+        const int vb = px(x, T - 1);
+        sB = __ballot_sync(~0u, g.th == T && (px(x - 1, T) == vb ||
+                                              px(x, T) == vb ||
+                                              px(x + 1, T) == vb));
+        const int y = lane;
+        const int vl = px(0, y);
+        sLc = __ballot_sync(~0u, y < g.th && (px(-1, y - 1) == vl ||
+                                              px(-1, y) == vl ||
+                                              px(-1, y + 1) == vl));
+        const int vr = px(T - 1, y);
+        sRc = __ballot_sync(~0u, g.tw == T && (px(T, y - 1) == vr ||
+                                               px(T, y) == vr ||
+                                               px(T, y + 1) == vr));
+    }
+
+    // -- per row (lane y): runs, seam and dead pixels --------------------------
+    const int y = lane;
+    // Shuffles run on every lane; lane 0 then drops the value it read back.
+    uint32_t Lm1 = __shfl_up_sync(~0u, rL, 1);
+    if (y == 0) {
+        Lm1 = 0u;
+    }
+    uint32_t Lp1 = __shfl_down_sync(~0u, rL, 1);
+    uint32_t EUp1 = __shfl_down_sync(~0u, rEU, 1);
+    uint32_t EULp1 = __shfl_down_sync(~0u, rEUL, 1);
+    uint32_t EURp1 = __shfl_down_sync(~0u, rEUR, 1);
+    if (y + 1 >= g.th) {
+        Lp1 = EUp1 = EULp1 = EURp1 = 0u;
+    }
+    const uint32_t cont = rEL & rL & (rL << 1);
+    const uint32_t heads = rL & ~cont;
+    const uint32_t ends = rL & ~(cont >> 1);
+    const uint32_t seam =
+        rL & ((y == 0 ? sT : 0u) | (y == T - 1 ? sB : 0u) |
+              ((sLc >> y) & 1u) | (((sRc >> y) & 1u) << 31));
+    uint32_t dead = (rEL & ~(rL << 1) & ~1u) | ((rEL >> 1) & ~(rL >> 1)) |
+                    (EUp1 & ~Lp1) | ((EURp1 << 1) & ~(Lp1 << 1)) |
+                    ((EULp1 >> 1) & ~(Lp1 >> 1));
+    if (y > 0) {
+        dead |= (rEU & ~Lm1) | (rEUL & ~(Lm1 << 1) & ~1u) |
+                (rEUR & ~(Lm1 >> 1) & 0x7FFFFFFFu);
+    }
+    dead &= rL;
+
+    // -- links: one union per contact of equal runs in rows y - 1 and y -------
+    volatile uint32_t* vw = sm.word;
+    {
+        uint32_t headsm1 = __shfl_up_sync(~0u, heads, 1);
+        if (y == 0) {
+            headsm1 = 0u;
+        }
+        const uint32_t eqlU = rEU & rL & Lm1;
+        const uint32_t eqlUL = rEUL & rL & (Lm1 << 1);
+        const uint32_t eqlUR = rEUR & rL & (Lm1 >> 1);
+        const uint32_t A = eqlU & ~eqlUL;            // partner (x, y - 1)
+        const uint32_t B = heads & eqlUL;            // partner (x - 1, y - 1)
+        const uint32_t C = ends & eqlUR & ~eqlU;     // partner (x + 1, y - 1)
+        uint32_t m = A | B | C;
+        while (__any_sync(~0u, m != 0u)) {
+            if (m) {
+                const int x = __ffs(m) - 1;
+                m &= m - 1u;
+                const int p = run_word(y, head_of(heads, x));
+                if (((A | B) >> x) & 1u) {
+                    const int xp = ((A >> x) & 1u) ? x : x - 1;
+                    runion(sm.word, p, run_word(y - 1, head_of(headsm1, xp)),
+                           err);
+                }
+                if ((C >> x) & 1u) {
+                    runion(sm.word, p,
+                           run_word(y - 1, head_of(headsm1, x + 1)), err);
+                }
+            }
+        }
+    }
+    __syncwarp();
+
+    // -- flatten; zone flags ORed into the roots --------------------------------
+    {
+        uint32_t r = heads;
+        while (__any_sync(~0u, r != 0u)) {
+            if (r) {
+                const int h = __ffs(r) - 1;
+                r &= r - 1u;
+                const int e = __ffs(ends & ~((1u << h) - 1u)) - 1;
+                const uint32_t R = range_mask(h, e);
+                const uint32_t own = ((rGT & R) ? kHasGreater : 0u) |
+                                     ((rLT & R) ? kHasSmaller : 0u) |
+                                     ((dead & R) ? kDead : 0u) |
+                                     ((seam & R) ? kTouchesSeam : 0u);
+                const int p = run_word(y, h);
+                int root = p;
+#pragma unroll 1
+                for (int it = 0; it < T * T; ++it) {
+                    const int up = rparent(vw[root], root);
+                    if (up == root) break;
+                    root = up;
+                }
+                if (root != p) {
+                    // p is not a root: no other lane writes its word now.
+                    vw[p] = with_parent(vw[p], p, root);
+                }
+                const uint32_t zf = (vw[root] >> kZoneShift) & 7u;
+                if ((zf & own) != own) {
+                    atomicOr(sm.word + root, own << kZoneShift);
+                }
+            }
+        }
+    }
+    __syncwarp();
+
+    // -- records of live seam zones, in pixel order ----------------------------
+    uint32_t live_roots = 0u;
+    {
+        uint32_t r = heads;
+        while (r) {
+            const int h = __ffs(r) - 1;
+            r &= r - 1u;
+            const int p = run_word(y, h);
+            const uint32_t w = vw[p];
+            const uint32_t z = (w >> kZoneShift) & 7u;
+            if (rparent(w, p) == p && (z & kTouchesSeam) &&
+                (z & kDead) != kDead) {
+                live_roots |= 1u << h;
+            }
+        }
+    }
+    uint32_t nrec = 0;
+    const uint32_t rec0 = warp_prefix(__popc(live_roots), nrec);
+    const int64_t frag_base = item * kSlots;
+    {
+        uint32_t r = live_roots;
+        uint32_t rec = rec0;
+        while (r) {
+            const int h = __ffs(r) - 1;
+            r &= r - 1u;
+            const int p = run_word(y, h);
+            if (rec < static_cast<uint32_t>(kSlots)) {
+                const uint32_t w = vw[p];
+                vw[p] = w | ((rec + 1u) << kRecShift);
+                const uint32_t z = (w >> kZoneShift) & 3u;
+                const int64_t gi = frag_base + rec;
+                a.parent[gi] = static_cast<int32_t>(gi);
+                a.bits[gi] = z | (z << kLocalShift);
+            } else {
+                err = kErrFragmentOverflow;
+            }
+            ++rec;
+        }
+    }
+    __syncwarp();
+
+    // -- listed pixels: verdicts of settled zones, run log of live zones ------
+    // Per row (lane y): `vmax` / `vmin` hold the listed pixels of settled
+    // zones whose maxima / minima byte is 255.
+    uint32_t* plog = a.pending + item * kPendingCap;
+    uint32_t vmax = 0u, vmin = 0u;
+    int nlog = 0;
+    {
+        uint32_t r = heads;
+        while (__any_sync(~0u, r != 0u)) {
+            bool logged = false;
+            uint32_t entry = 0u;
+            if (r) {
+                const int h = __ffs(r) - 1;
+                r &= r - 1u;
+                const int e = __ffs(ends & ~((1u << h) - 1u)) - 1;
+                const uint32_t R = range_mask(h, e);
+                const int p = run_word(y, h);
+                const int root = rparent(vw[p], p);
+                const uint32_t w = vw[root];
+                const uint32_t z = (w >> kZoneShift) & 7u;
+                const bool live = (z & kTouchesSeam) && (z & kDead) != kDead;
+                if (live) {
+                    const uint32_t rec1 = (w >> kRecShift) & 0xFFu;
+                    if (rec1) {
+                        logged = true;
+                        entry = pending_entry(static_cast<int>(rec1 - 1u), h,
+                                              y, e - h + 1);
+                    }
+                } else {
+                    vmax |= (z & kHasGreater) ? 0u : R;
+                    vmin |= (z & kHasSmaller) ? 0u : R;
+                }
+            }
+            const uint32_t bal = __ballot_sync(~0u, logged);
+            if (logged) {
+                plog[nlog + __popc(bal & lt_mask)] = entry;
+            }
+            nlog += __popc(bal);
+        }
+    }
+    // The mask bytes of every pixel of the tile.  Pixels of live zones get a
+    // placeholder 0 here and their final bytes from the resolve pass, which
+    // runs after this pass; so whole rows are written, with 16-, 8- or
+    // 4-byte stores where the output rows allow it.
+    {
+        const uint64_t bmx = reinterpret_cast<uint64_t>(
+            omax + static_cast<int64_t>(g.y0) * out_pitch + g.x0);
+        const uint64_t bmn = reinterpret_cast<uint64_t>(
+            omin + static_cast<int64_t>(g.y0) * out_pitch + g.x0);
+        const uint64_t align = bmx | bmn | static_cast<uint64_t>(out_pitch);
+        int vec = (align & 15u) == 0 ? 16 : (align & 7u) == 0 ? 8
+                : (align & 3u) == 0 ? 4 : 1;
+        if (g.tw < T || g.th < T) {
+            vec = 1;
+        }
+        if (vec > 1) {
+            store_rows(omax, omin, g, out_pitch, vmax, vmin, vec);
+        } else {
+            uint8_t* pmx = omax + static_cast<int64_t>(g.y0) * out_pitch +
+                           g.x0 + lane;
+            uint8_t* pmn = omin + static_cast<int64_t>(g.y0) * out_pitch +
+                           g.x0 + lane;
+#pragma unroll 2
+            for (int yy = 0; yy < g.th; ++yy) {
+                const uint32_t mxr = __shfl_sync(~0u, vmax, yy);
+                const uint32_t mnr = __shfl_sync(~0u, vmin, yy);
+                if (col_ok) {
+                    *pmx = ((mxr >> lane) & 1u) ? 255 : 0;
+                    *pmn = ((mnr >> lane) & 1u) ? 255 : 0;
+                }
+                pmx += out_pitch;
+                pmn += out_pitch;
+            }
+        }
+    }
+
+    // -- border records, seam items ---------------------------------------------
+    uint8_t* border = a.border + item * kSlots;
+    // Record of tile pixel (x, yy) whose row has listed mask `lrow` and run
+    // heads `hrow`.
+    auto record_of = [&](int x, int yy, uint32_t lrow,
+                         uint32_t hrow) -> uint32_t {
+        if (!((lrow >> x) & 1u)) {
+            return kDeadRecord;   // a decided pixel
+        }
+        const int p = run_word(yy, head_of(hrow, x));
+        const int root = rparent(vw[p], p);
+        const uint32_t w = vw[root];
+        const uint32_t z = (w >> kZoneShift) & 7u;
+        if ((z & kDead) == kDead) {
+            return kDeadRecord;
+        }
+        const uint32_t r1 = (w >> kRecShift) & 0xFFu;
+        return r1 ? r1 - 1u : kNoRecord;
+    };
+    uint32_t* items = a.seam_items + item * kSeamCap;
+    int nitems = 0;
+    auto emit = [&](bool ok, uint32_t rec, int dir, int off) {
+        const uint32_t bal = __ballot_sync(~0u, ok);
+        if (ok) {
+            items[nitems + __popc(bal & lt_mask)] =
+                rec | (static_cast<uint32_t>(off) << 8) |
+                (static_cast<uint32_t>(dir) << 16);
+        }
+        nitems += __popc(bal);
+    };
+    {
+        const uint32_t l_top = __shfl_sync(~0u, rL, 0);
+        const uint32_t h_top = __shfl_sync(~0u, heads, 0);
+        const uint32_t l_bot = __shfl_sync(~0u, rL, g.th - 1);
+        const uint32_t h_bot = __shfl_sync(~0u, heads, g.th - 1);
+        const int x = lane;
+        const bool in_row = x < g.tw;
+        const uint32_t rt = in_row ? record_of(x, 0, l_top, h_top) : kNoRecord;
+        const uint32_t rb =
+            in_row ? record_of(x, g.th - 1, l_bot, h_bot) : kNoRecord;
+        if (in_row) {
+            border[x] = static_cast<uint8_t>(rt);
+            border[T + x] = static_cast<uint8_t>(rb);
+        }
+        const bool live_t = rt < static_cast<uint32_t>(kSlots);
+        const bool live_b = rb < static_cast<uint32_t>(kSlots) &&
+                            g.th == T && g.y0 + T < height;
+        const int vt = px(x, 0);
+        const int vb = px(x, T - 1);
+#pragma unroll
+        for (int d = -1; d <= 1; ++d) {
+            const int x2 = x + d;
+            const int dir_t = x2 < 0 ? kRelTopLeft
+                                     : (x2 >= T ? kRelTopRight : kRelTop);
+            const int off_t = T + (x2 < 0 ? T - 1 : (x2 >= T ? 0 : x2));
+            emit(live_t && px(x2, -1) == vt, rt, dir_t, off_t);
+            const int dir_b = x2 < 0 ? kRelBottomLeft
+                                     : (x2 >= T ? kRelBottomRight : kRelBottom);
+            const int off_b = x2 < 0 ? T - 1 : (x2 >= T ? 0 : x2);
+            emit(live_b && px(x2, T) == vb, rb, dir_b, off_b);
+        }
+    }
+    {
+        const bool in_col = y < g.th;
+        const uint32_t rl = in_col ? record_of(0, y, rL, heads) : kNoRecord;
+        const uint32_t rr =
+            in_col ? record_of(g.tw - 1, y, rL, heads) : kNoRecord;
+        if (in_col) {
+            border[2 * T + y] = static_cast<uint8_t>(rl);
+            border[3 * T + y] = static_cast<uint8_t>(rr);
+        }
+        const bool live_l = rl < static_cast<uint32_t>(kSlots);
+        const bool live_r = rr < static_cast<uint32_t>(kSlots) &&
+                            g.tw == T && g.x0 + T < width;
+        const int vl = px(0, y);
+        const int vr = px(T - 1, y);
+#pragma unroll
+        for (int d = -1; d <= 1; ++d) {
+            const int y2 = y + d;
+            const bool inside = y2 >= 0 && y2 < g.th;   // corners: rows above
+            emit(live_l && inside && px(-1, y2) == vl, rl, kRelLeft,
+                 3 * T + y2);
+            emit(live_r && inside && px(T, y2) == vr, rr, kRelRight,
+                 2 * T + y2);
+        }
+    }
+    if (lane == 0) {
+        a.fragment_count[item] =
+            static_cast<uint16_t>(min(nrec, static_cast<uint32_t>(kSlots)));
+        a.pending_count[item] = static_cast<uint32_t>(nlog);
+        a.seam_count[item] = static_cast<uint32_t>(nitems);
+    }
+    if (err) {
+        raise_error(a.header, err, static_cast<uint32_t>(item));
+    }
+}
+
+}  // namespace rowscan
+
+}  // namespace ss
