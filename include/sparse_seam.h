@@ -122,10 +122,9 @@ typedef struct ss_stats {
  * process (the autotuner's hook; the masks never depend on it).
  *   warps > 0   CTA-per-tile kernels with `warps` warps per CTA
  *               (tile 16: 2, 4 or 8; tile 32: 4, 8 or 16; tile 64: 8 or 16)
- *   warps < 0   tile 32 only: row-scan kernels, one tile per warp: -2 / -4
- *               (per-pixel list of the listed pixels, 2 / 4 warps per CTA)
- *               or -18 / -20 (per-row masks and runs, 2 / 4 warps per CTA)
- * Defaults: tile 16 -> 4, tile 32 -> -4, tile 64 -> 16.  The reference fixes
+ *   warps < 0   tile 32 only: row-scan kernels (per-row bit masks and runs),
+ *               one tile per warp, -warps warps per CTA (2 or 4)
+ * Defaults: tile 16 -> 4, tile 32 -> -2, tile 64 -> 16.  The reference fixes
  * its tile and classify threads at compile time
  * (harness/configuration_study/sparse_config_benchmark_v0_8.cu:17-30). */
 ss_status ss_set_kernel_config(int tile, int warps);

@@ -433,44 +433,7 @@ __global__ void init_header_kernel(Header* h) {
 // Row-scan kernels (T = 32): NW independent warps per CTA, one tile each.
 // ---------------------------------------------------------------------------
 
-template <int NW, bool kPersistent>
-__global__ void __launch_bounds__(NW * 32)
-rowscan_tile_pass_kernel(Source src, Arena a) {
-    __shared__ rowscan::WarpSmem sm[NW];
-    const int warp = static_cast<int>(threadIdx.x) >> 5;
-    const int lane = static_cast<int>(threadIdx.x) & 31;
-    if (a.header->magic != kMagic) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            raise_error(a.header, kErrUninitialized, 0u);
-        }
-        return;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        a.header->last_tiles = static_cast<uint64_t>(src.total_tiles);
-        a.header->tile = rowscan::T;
-    }
-    if constexpr (kPersistent) {
-        for (;;) {
-            uint32_t item = 0;
-            if (lane == 0) {
-                item = atomicAdd(&a.header->queue_head, 1u);
-            }
-            item = __shfl_sync(~0u, item, 0);
-            if (static_cast<int64_t>(item) >= src.total_tiles) {
-                break;
-            }
-            rowscan::tile_pass_warp(sm[warp], src, a, item);
-            __syncwarp();
-        }
-    } else {
-        const int64_t item = static_cast<int64_t>(blockIdx.x) * NW + warp;
-        if (item < src.total_tiles) {
-            rowscan::tile_pass_warp(sm[warp], src, a, item);
-        }
-    }
-}
-
-// Run-mask variant of the tile pass (same contract, same later passes).
+// Row-scan tile pass: NW independent warps per CTA, one tile each.
 template <int NW, bool kPersistent>
 __global__ void __launch_bounds__(NW * 32)
 runs_tile_pass_kernel(Source src, Arena a) {
@@ -708,18 +671,6 @@ struct Config {
 #define SS_ROWSCAN(NW)                                                        \
     Config {                                                                  \
         32, -(NW),                                                            \
-            {rowscan_tile_pass_kernel<NW, false>,                             \
-             rowscan_tile_pass_kernel<NW, true>},                             \
-            {rowscan_resolve_pass_kernel<NW, false>,                          \
-             rowscan_resolve_pass_kernel<NW, true>}, NW,                      \
-            rowscan_seam_pass_kernel<NW, false>, 32 * NW,                     \
-            rowscan_flags_pass_kernel<NW>                                     \
-    }
-
-// Run-mask row-scan configurations are listed with warps = -(16 + NW).
-#define SS_RUNS(NW)                                                           \
-    Config {                                                                  \
-        32, -(16 + (NW)),                                                     \
             {runs_tile_pass_kernel<NW, false>,                                \
              runs_tile_pass_kernel<NW, true>},                                \
             {rowscan_resolve_pass_kernel<NW, false>,                          \
@@ -732,15 +683,14 @@ static const Config kConfigs[] = {
     SS_CONFIG(16, 2), SS_CONFIG(16, 4), SS_CONFIG(16, 8),
     SS_CONFIG(32, 4), SS_CONFIG(32, 8), SS_CONFIG(32, 16),
     SS_CONFIG(64, 8), SS_CONFIG(64, 16),
-    SS_ROWSCAN(2), SS_ROWSCAN(4), SS_RUNS(2), SS_RUNS(4),
+    SS_ROWSCAN(2), SS_ROWSCAN(4),
 };
 #undef SS_CONFIG
 #undef SS_ROWSCAN
-#undef SS_RUNS
 
 // Per tile size, the configuration used by default (index by tile / 16 - 1);
 // negative warps select the row-scan kernels.
-static std::atomic<int> g_default_warps[4] = {{4}, {-4}, {0}, {16}};
+static std::atomic<int> g_default_warps[4] = {{4}, {-2}, {0}, {16}};
 
 static const Config* find_config(int tile, int warps) {
     for (const Config& c : kConfigs) {
@@ -839,7 +789,7 @@ static ss_status launch_route(const Config& cfg, const Source& src_in,
     // the launches below.
     (void)cudaGetLastError();
     Source src = src_in;
-    const int nw = cfg.warps < 0 ? (-cfg.warps) % 16 : cfg.warps;
+    const int nw = cfg.warps < 0 ? -cfg.warps : cfg.warps;
     const int threads = nw * 32;
     // Tiles per CTA of the passes after the tile pass.
     int later_per_cta = cfg.later_per_cta;

@@ -1,14 +1,13 @@
-// ss_runs.cuh -- T = 32 tile pass on per-row bit masks and runs.
+// ss_runs.cuh -- the T = 32 tile pass: one warp per 32 x 32 tile, on
+// per-row bit masks and runs.
 //
-// Same contract as tile_pass_warp (ss_rowscan.cuh): one warp per 32 x 32
-// tile; the pixels other than "decided" ones (with both a greater and a
-// smaller 8-neighbour) are labelled into flat zones, live seam zones are
-// numbered and logged for the seam and resolve passes, and every pixel
-// outside a live zone gets its mask bytes in one final row pass (whole
-// 32-byte rows where the row holds no live pixel).  The difference is the representation of the
-// listed pixels: instead of a per-pixel list, the row scan leaves seven
-// 32-bit masks per tile row in the registers of lane y = row:
-//   L    listed pixels
+// The tile and its one-pixel halo are staged in shared memory (int16, -1
+// outside the image).  A row scan (lane = column) finds each pixel's
+// greater / smaller flags from sliding 3 x 3 maxima / minima (a signed max
+// and an unsigned min both ignore -1); "decided" pixels have both and are in
+// neither mask, with their whole zone.  The scan leaves seven 32-bit masks
+// per tile row in the registers of lane y = row:
+//   L    listed pixels (not decided)
 //   GT   listed pixels with a strictly greater 8-neighbour
 //   LT   listed pixels with a strictly smaller 8-neighbour
 //   EU   pixels equal to the pixel above          (bit x: v(x,y) == v(x,y-1))
@@ -21,11 +20,19 @@
 //             (their zone holds a decided pixel, so it is in no mask);
 //   seam      listed pixels with an equal neighbour outside the tile;
 //   links     one union per pair of 8-adjacent equal runs in consecutive
-//             rows, at the first column of their contact (three cases, as in
-//             tile_pass_warp's phase C).
+//             rows, at the first column of their contact: (a) a pixel equal
+//             to the one above and not to the one above-left, (b) a run head
+//             equal to the pixel above-left, (c) a run end equal to the pixel
+//             above-right and not to the one above.
 // Union-find runs over run heads only, one lane per row, so its cost grows
 // with the number of runs and contacts per row rather than with the number
-// of listed pixels: large plateaus cost a few runs per row.
+// of listed pixels: a large plateau is a few runs per row.  Zone flags are
+// ORed into the roots; live seam zones (touching a seam, flags not both set)
+// get records in pixel order of their roots and a log of their runs; every
+// pixel of the tile gets its mask bytes in one final pass, whole rows with
+// vector stores where the output allows (live pixels get a placeholder that
+// the resolve pass replaces); border records and seam items go to the
+// workspace for the seam pass.
 //
 // Reference behaviour followed (paths inside the reference repository):
 // zone flags and seam test, harness/primary/snapshot_sparse_seam_cuda_v1_0.cu
@@ -44,9 +51,8 @@ struct __align__(16) RunSmem {
     int16_t img[kHaloW * kHaloW];  // tile + halo, -1 outside the image
 };
 
-// Run-head words use the layout of the list kernels (bits 10-12 zone flags,
-// 13-20 record + 1) but store the parent as (parent XOR self) in bits 0-9,
-// so an all-zero word is a root with no flags: the words start zeroed.
+// Run-head words store the parent as (parent XOR self) in bits 0-9, so an
+// all-zero word is a root with no flags: the words start zeroed.
 __device__ __forceinline__ int rparent(uint32_t w, int x) {
     return static_cast<int>((w & kParMask) ^ static_cast<uint32_t>(x));
 }
@@ -162,7 +168,6 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                                                     int64_t item) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
     const uint32_t lt_mask = (1u << lane) - 1u;
-    const uint32_t le_mask = lt_mask | (1u << lane);
     uint32_t err = 0;
 
     const PlanImage job = load_job(src, item);

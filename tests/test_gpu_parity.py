@@ -14,8 +14,7 @@ pytestmark = pytest.mark.gpu
 
 TILES = (16, 32, 64)
 # (tile, kernel configuration): every kernel family the library ships.
-CONFIGS = [(16, 4), (16, 2), (32, -4), (32, -2), (32, -20), (32, -18),
-           (32, 8), (64, 16), (64, 8)]
+CONFIGS = [(16, 4), (16, 2), (32, -2), (32, -4), (32, 8), (64, 16), (64, 8)]
 
 
 @pytest.fixture
@@ -115,8 +114,8 @@ def test_config1_uniform_q16_and_constant():
     assert (got[0] == 255).all() and (got[1] == 255).all()
 
 
-@pytest.mark.parametrize("kernel_config", [(32, -4), (32, -20), (32, 8)],
-                         indirect=True, ids=["rowscan", "runs", "cta"])
+@pytest.mark.parametrize("kernel_config", [(32, -2), (32, -4), (32, 8)],
+                         indirect=True, ids=["rowscan2", "rowscan4", "cta"])
 def test_plateau_and_seam_heavy_families(kernel_config):
     import importlib
     synth = importlib.import_module("sparse-seam_b200.synth")
