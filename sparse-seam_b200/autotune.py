@@ -178,13 +178,16 @@ class TunedBatch:
     """A batch split by size class, each part launched with its tuned choice.
 
     Classes whose choices differ only in the seam/resolve grouping share one
-    launch (with the grouping chosen from that launch's tile count).  Parts
-    run one after another on one stream, so the whole batch can be captured
-    in one CUDA graph.
+    launch (with the grouping chosen from that launch's tile count).  The
+    parts run concurrently, each on its own stream forked from and joined
+    back into the caller's stream with events, so the GPU fills its SMs from
+    all parts at once; the fork and join are captured into a CUDA graph like
+    any other stream work.
     """
 
     def __init__(self, images: Sequence, maxima: Sequence, minima: Sequence,
                  table: TuningTable, stream=None):
+        import torch
         parts: Dict[Choice, List[int]] = {}
         groups: Dict[Tuple[int, int, bool], set] = {}
         for c in table.choices.values():
@@ -204,12 +207,29 @@ class TunedBatch:
                                   stream=stream)
             self.parts.append((choice, plan,
                                plan.make_workspace(stream=stream)))
+        device = images[0].device if len(images) else None
+        self._streams = [torch.cuda.Stream(device)
+                         for _ in self.parts[1:]]
 
     def run(self, stream=None) -> None:
-        for choice, plan, ws in self.parts:
+        import torch
+        main = stream or torch.cuda.current_stream()
+        fork = torch.cuda.Event()
+        fork.record(main)
+        joins = []
+        for i, (choice, plan, ws) in enumerate(self.parts):
+            st = main if i == 0 else self._streams[i - 1]
+            if i:
+                st.wait_event(fork)
             plan.run_launch(ws, warps=choice.warps,
                             persistent=choice.persistent, group=choice.group,
-                            stream=stream)
+                            stream=st)
+            if i:
+                done = torch.cuda.Event()
+                done.record(st)
+                joins.append(done)
+        for done in joins:
+            main.wait_event(done)
 
     def read_status(self, stream=None) -> None:
         for _, _, ws in self.parts:
