@@ -251,6 +251,30 @@ ss_status ss_extrema_batch_launch(const void* h_plan, const void* d_plan,
                                   void* stream);
 
 /* ---------------------------------------------------------------------- */
+/* Compact host-to-host transfer of the masks.                              */
+/* ---------------------------------------------------------------------- */
+/* Host-to-host throughput is bound by the bus: 1 byte per pixel goes in and
+ * two mask bytes come back.  ss_pack_masks packs `n` consecutive mask bytes
+ * of each mask (any non-zero byte = 1) into bit planes on the device, bit i
+ * of word i / 32 for pixel i, (n + 31) / 32 words each; after the planes are
+ * copied to the host, ss_unpack_masks writes the 0/255 bytes into the host
+ * masks with `threads` host threads (0 = all), and ss_enqueue_unpack_masks
+ * does the same as a host function enqueued on `stream` (ordered after the
+ * stream's earlier work; the buffers must stay valid until it runs).  No
+ * counterpart in the reference, which copies both byte masks back
+ * (harness/primary/gpu_common_v0_6.cu:351-373). */
+ss_status ss_pack_masks(const uint8_t* d_maxima, const uint8_t* d_minima,
+                        uint64_t n, uint32_t* d_max_bits,
+                        uint32_t* d_min_bits, void* stream);
+ss_status ss_unpack_masks(const uint32_t* h_max_bits,
+                          const uint32_t* h_min_bits, uint64_t n,
+                          uint8_t* h_maxima, uint8_t* h_minima, int threads);
+ss_status ss_enqueue_unpack_masks(const uint32_t* h_max_bits,
+                                  const uint32_t* h_min_bits, uint64_t n,
+                                  uint8_t* h_maxima, uint8_t* h_minima,
+                                  int threads, void* stream);
+
+/* ---------------------------------------------------------------------- */
 /* Serving: a continuous-batching request loop on one GPU.                 */
 /* ---------------------------------------------------------------------- */
 /* No counterpart in the reference, whose harness runs one image at a time

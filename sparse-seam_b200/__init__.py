@@ -188,6 +188,10 @@ SIGNATURES = {
                             ctypes.POINTER(_I), _I]),
     "ss_server_get_stats": (_I, [_VP, ctypes.POINTER(ServerStats)]),
     "ss_server_destroy": (None, [_VP]),
+    "ss_pack_masks": (_I, [_VP, _VP, ctypes.c_uint64, _VP, _VP, _VP]),
+    "ss_unpack_masks": (_I, [_VP, _VP, ctypes.c_uint64, _VP, _VP, _I]),
+    "ss_enqueue_unpack_masks": (_I, [_VP, _VP, ctypes.c_uint64, _VP, _VP, _I,
+                                     _VP]),
 }
 
 

@@ -1,7 +1,8 @@
 """Build recipe for the CUDA route library (sm_100a).
 
-Compiles ``csrc/ss_route.cu`` (the route) and ``csrc/ss_server.cu`` (the
-serving loop) into ``libsparseseam.so`` next to this file with
+Compiles ``csrc/ss_route.cu`` (the route), ``csrc/ss_server.cu`` (the
+serving loop) and ``csrc/ss_pack.cu`` (compact mask transfer, host side with
+OpenMP) into ``libsparseseam.so`` next to this file with
 nvcc.  The library has a plain C ABI (``include/sparse_seam.h``) and links the
 CUDA runtime statically, so it loads into any process on the GPU host, with or
 without PyTorch.
@@ -16,11 +17,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 INCLUDE = os.path.join(ROOT, "include")
 SOURCES = [os.path.join(HERE, "csrc", "ss_route.cu"),
-           os.path.join(HERE, "csrc", "ss_server.cu")]
+           os.path.join(HERE, "csrc", "ss_server.cu"),
+           os.path.join(HERE, "csrc", "ss_pack.cu")]
 DEPENDS = SOURCES + [
     os.path.join(HERE, "csrc", name)
     for name in ("ss_device.cuh", "ss_tile.cuh", "ss_rowscan.cuh",
-                 "ss_internal.h", "ss_pool.hpp")
+                 "ss_runs.cuh", "ss_internal.h", "ss_pool.hpp")
 ] + [os.path.join(INCLUDE, "sparse_seam.h")]
 LIBRARY = os.path.join(HERE, "libsparseseam.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -37,9 +39,9 @@ def nvcc() -> str:
 def command(output: str, extra=()) -> list:
     return [
         nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17",
-        "-I" + INCLUDE, "-Xcompiler", "-fPIC", "-shared",
-        "-Xptxas", "-warn-spills",
-        *extra, "-o", output, *SOURCES,
+        "-I" + INCLUDE, "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp",
+        "-shared", "-Xptxas", "-warn-spills",
+        *extra, "-o", output, *SOURCES, "-lgomp",
     ]
 
 

@@ -4,9 +4,13 @@ The reference times a host-to-host form per image (H2D of the image, the
 route, D2H of both masks; harness/primary/gpu_common_v0_6.cu:351-373).  Here a
 corpus of host images is cut into chunks; each chunk's images are packed into
 one pinned buffer and copied with a single cudaMemcpyAsync on a copy stream,
-run as one batch on the compute stream, and both masks come back with one
-copy each on a read-back stream, so the H2D of chunk c+1, the kernels of
-chunk c and the D2H of chunk c-1 overlap.
+and run as one batch on the compute stream.  The masks come back on a
+read-back stream, so the H2D of chunk c+1, the kernels of chunk c and the D2H
+of chunk c-1 overlap.  With `packed` (the default) the device packs both
+masks into bit planes (ss_pack_masks), only the planes cross the bus (0.25
+instead of 2 bytes per pixel), and a host function enqueued on a fourth
+stream expands them into the pinned byte masks with all host threads
+(ss_enqueue_unpack_masks), overlapping the transfers of the next chunks.
 """
 from __future__ import annotations
 
@@ -25,7 +29,8 @@ class HostBatch:
     """
 
     def __init__(self, images: Sequence[np.ndarray], tile: int = 32,
-                 chunks: int = 4, persistent: bool = False, device=None):
+                 chunks: int = 4, persistent: bool = False, device=None,
+                 packed: bool = True, threads: int = 0):
         import torch
         from importlib import import_module
         self._pkg = import_module("sparse-seam_b200")
@@ -84,6 +89,21 @@ class HostBatch:
         self.copy_in = torch.cuda.Stream(device=self.device)
         self.compute = torch.cuda.Stream(device=self.device)
         self.copy_out = torch.cuda.Stream(device=self.device)
+        self.packed = packed
+        self.threads = int(threads)
+        if packed:
+            # Bit planes: per chunk (hi - lo + 31) // 32 words per mask.
+            self.words = []
+            w0 = 0
+            for lo, hi, _ in self.chunks:
+                n_words = (hi - lo + 31) // 32
+                self.words.append((w0, n_words))
+                w0 += n_words
+            self.d_bits = torch.empty((2, max(w0, 1)), dtype=torch.int32,
+                                      device=self.device)
+            self.h_bits = torch.empty((2, max(w0, 1)), dtype=torch.int32,
+                                      pin_memory=True)
+            self.unpack = torch.cuda.Stream(device=self.device)
         torch.cuda.synchronize(self.device)
 
     @property
@@ -92,6 +112,8 @@ class HostBatch:
 
     @property
     def d2h_bytes(self) -> int:
+        if self.packed:
+            return 2 * 4 * sum(n for _, n in self.words)
         return 2 * self.pixels
 
     def run(self, start_stream=None):
@@ -108,7 +130,10 @@ class HostBatch:
         self.copy_in.wait_event(begin)
         self.compute.wait_event(begin)
         self.copy_out.wait_event(begin)
-        for lo, hi, plan in self.chunks:
+        if self.packed:
+            self.unpack.wait_event(begin)
+        lib = self._pkg.lib()
+        for c, (lo, hi, plan) in enumerate(self.chunks):
             with torch.cuda.stream(self.copy_in):
                 self.d_in[lo:hi].copy_(self.h_in[lo:hi], non_blocking=True)
                 loaded = torch.cuda.Event()
@@ -116,14 +141,39 @@ class HostBatch:
             self.compute.wait_event(loaded)
             plan.run(self.workspace, persistent=self.persistent,
                      stream=self.compute)
+            if self.packed:
+                w0, nw = self.words[c]
+                d_mx = self.d_bits[0, w0:w0 + nw]
+                d_mn = self.d_bits[1, w0:w0 + nw]
+                self._pkg._check(lib.ss_pack_masks(
+                    self.d_max[lo:hi].data_ptr(),
+                    self.d_min[lo:hi].data_ptr(), hi - lo, d_mx.data_ptr(),
+                    d_mn.data_ptr(),
+                    self._pkg._stream_handle(self.compute)), "ss_pack_masks")
             done = torch.cuda.Event()
             done.record(self.compute)
             self.copy_out.wait_event(done)
             with torch.cuda.stream(self.copy_out):
-                self.h_max[lo:hi].copy_(self.d_max[lo:hi], non_blocking=True)
-                self.h_min[lo:hi].copy_(self.d_min[lo:hi], non_blocking=True)
+                if self.packed:
+                    self.h_bits[0, w0:w0 + nw].copy_(d_mx, non_blocking=True)
+                    self.h_bits[1, w0:w0 + nw].copy_(d_mn, non_blocking=True)
+                    arrived = torch.cuda.Event()
+                    arrived.record(self.copy_out)
+                else:
+                    self.h_max[lo:hi].copy_(self.d_max[lo:hi],
+                                            non_blocking=True)
+                    self.h_min[lo:hi].copy_(self.d_min[lo:hi],
+                                            non_blocking=True)
+            if self.packed:
+                self.unpack.wait_event(arrived)
+                self._pkg._check(lib.ss_enqueue_unpack_masks(
+                    self.h_bits[0, w0:].data_ptr(),
+                    self.h_bits[1, w0:].data_ptr(), hi - lo,
+                    self.h_max[lo:hi].data_ptr(), self.h_min[lo:hi].data_ptr(),
+                    self.threads, self._pkg._stream_handle(self.unpack)),
+                    "ss_enqueue_unpack_masks")
         end = torch.cuda.Event(enable_timing=True)
-        end.record(self.copy_out)
+        end.record(self.unpack if self.packed else self.copy_out)
         # The next pass may reuse the device buffers only after this one.
         start_stream.wait_event(end)
         return end

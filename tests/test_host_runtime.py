@@ -93,3 +93,54 @@ def test_autotuner_tables():
     back = at.TuningTable.from_json(table.to_json())
     assert back.choices == table.choices
     assert back.choice_for(700, 700) == cands[3]
+
+
+def test_unpack_masks_on_the_host():
+    """The host half of the compact transfer: bit planes (bit i of word
+    i / 32 for pixel i) back to 0/255 bytes, any length, any thread count."""
+    import numpy as np
+    pkg = package()
+    lib = pkg.lib()
+    rng = np.random.default_rng(4)
+    for n in (0, 1, 7, 15, 16, 17, 31, 32, 33, 47, 1000, 65536,
+              65536 * 3 + 17, 65536 * 2 + 31):
+        want_max = (rng.random(n) < 0.3).astype(np.uint8) * 255
+        want_min = (rng.random(n) < 0.6).astype(np.uint8) * 255
+        words = (n + 31) // 32
+        bmax = np.zeros(words * 4, np.uint8)
+        bmin = np.zeros(words * 4, np.uint8)
+        pm = np.packbits(want_max != 0, bitorder="little")
+        pn = np.packbits(want_min != 0, bitorder="little")
+        bmax[:pm.size] = pm
+        bmin[:pn.size] = pn
+        for threads, shift in ((1, 0), (3, 5), (0, 13), (2, 1)):
+            # Outputs at every alignment: the streaming middle and the
+            # byte-wise head and tail must join up.
+            buf_max = np.full(n + 40, 9, np.uint8)
+            buf_min = np.full(n + 40, 9, np.uint8)
+            out_max = buf_max[shift:shift + n + 5]
+            out_min = buf_min[shift:shift + n + 5]
+            assert lib.ss_unpack_masks(bmax.ctypes.data, bmin.ctypes.data, n,
+                                       out_max.ctypes.data,
+                                       out_min.ctypes.data, threads) == 0
+            assert np.array_equal(out_max[:n], want_max), (n, threads, shift)
+            assert np.array_equal(out_min[:n], want_min), (n, threads, shift)
+            assert (out_max[n:] == 9).all() and (out_min[n:] == 9).all()
+            assert (buf_max[:shift] == 9).all()
+    assert lib.ss_unpack_masks(None, None, 4, None, None, 1) == 1
+
+
+@pytest.mark.parametrize("simd", ["0", "1", "2"])
+def test_unpack_masks_every_simd_path(simd):
+    """The scalar, AVX2 and AVX-512 expansions (as far as this CPU has them)
+    agree with numpy, run in a child process with the level capped."""
+    import sys
+    code = (
+        "import sys; sys.path.insert(0, %r); sys.path.insert(0, %r)\n"
+        "import test_host_runtime as t\n"
+        "t.test_unpack_masks_on_the_host()\n"
+        "print('OK')\n" % (ROOT, os.path.join(ROOT, "tests")))
+    env = dict(os.environ, SS_UNPACK_SIMD=simd)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True,
+                         text=True, timeout=300, env=env, cwd=ROOT)
+    assert out.returncode == 0 and "OK" in out.stdout, out.stderr[-2000:]
