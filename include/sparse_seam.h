@@ -258,7 +258,8 @@ ss_status ss_extrema_batch_launch(const void* h_plan, const void* d_plan,
  * of each mask (any non-zero byte = 1) into bit planes on the device, bit i
  * of word i / 32 for pixel i, (n + 31) / 32 words each; after the planes are
  * copied to the host, ss_unpack_masks writes the 0/255 bytes into the host
- * masks with `threads` host threads (0 = all), and ss_enqueue_unpack_masks
+ * masks with `threads` host threads (0 = all processors but one), and
+ * ss_enqueue_unpack_masks
  * does the same as a host function enqueued on `stream` (ordered after the
  * stream's earlier work; the buffers must stay valid until it runs).  No
  * counterpart in the reference, which copies both byte masks back

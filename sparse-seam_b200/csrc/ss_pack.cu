@@ -224,6 +224,18 @@ static void expand_best(const uint32_t* bits, uint64_t n, uint8_t* out,
     expand(bits, n, out, t);
 }
 
+// Threads for an unpack: the caller's choice, else all processors but one
+// (the thread that waits for the GPU or feeds it keeps a core; with every
+// core busy expanding, the waiting thread and the runtime's own threads
+// preempt the expansion threads and the unpack slows several-fold).
+static int unpack_threads(int threads) {
+    if (threads > 0) {
+        return threads;
+    }
+    const int procs = omp_get_num_procs();
+    return procs > 1 ? procs - 1 : 1;
+}
+
 struct UnpackJob {
     const uint32_t* max_bits;
     const uint32_t* min_bits;
@@ -297,7 +309,7 @@ ss_status ss_unpack_masks(const uint32_t* h_max_bits,
         return SS_ERR_INVALID_VALUE;
     }
     UnpackJob j{h_max_bits, h_min_bits, n, h_maxima, h_minima,
-                threads > 0 ? threads : omp_get_max_threads()};
+                unpack_threads(threads)};
     unpack(j);
     return SS_OK;
 }
@@ -311,7 +323,7 @@ ss_status ss_enqueue_unpack_masks(const uint32_t* h_max_bits,
     }
     UnpackJob* j = new (std::nothrow)
         UnpackJob{h_max_bits, h_min_bits, n, h_maxima, h_minima,
-                  threads > 0 ? threads : omp_get_max_threads()};
+                  unpack_threads(threads)};
     if (!j) {
         return SS_ERR_HOST_ALLOC;
     }
