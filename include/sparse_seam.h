@@ -276,6 +276,22 @@ ss_status ss_enqueue_unpack_masks(const uint32_t* h_max_bits,
                                   int threads, void* stream);
 
 /* ---------------------------------------------------------------------- */
+/* Image files.                                                            */
+/* ---------------------------------------------------------------------- */
+/* Reads a PGM (P5 / P2, maxval <= 255) or PNG (any colour type, 1/2/4/8-bit
+ * samples, not interlaced) as 8-bit gray, as the reference's
+ * cv::imread(path, IMREAD_GRAYSCALE) does
+ * (harness/primary/snapshot_sparse_seam_cuda_v1_0.cu:87-103).  With `pixels`
+ * NULL only `width` and `height` are filled; otherwise `capacity` must hold
+ * width * height bytes (rows packed).  SS_ERR_INVALID_VALUE for an unreadable
+ * or unsupported file. */
+ss_status ss_read_image(const char* path, uint8_t* pixels, size_t capacity,
+                        int* width, int* height);
+/* Writes a binary PGM (P5, maxval 255). */
+ss_status ss_write_pgm(const char* path, const uint8_t* pixels, int width,
+                       int height, int pitch);
+
+/* ---------------------------------------------------------------------- */
 /* Serving: a continuous-batching request loop on one GPU.                 */
 /* ---------------------------------------------------------------------- */
 /* No counterpart in the reference, whose harness runs one image at a time

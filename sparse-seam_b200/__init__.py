@@ -192,7 +192,31 @@ SIGNATURES = {
     "ss_unpack_masks": (_I, [_VP, _VP, ctypes.c_uint64, _VP, _VP, _I]),
     "ss_enqueue_unpack_masks": (_I, [_VP, _VP, ctypes.c_uint64, _VP, _VP, _I,
                                      _VP]),
+    "ss_read_image": (_I, [ctypes.c_char_p, _VP, _SZ, ctypes.POINTER(_I),
+                           ctypes.POINTER(_I)]),
+    "ss_write_pgm": (_I, [ctypes.c_char_p, _VP, _I, _I, _I]),
 }
+
+
+def read_image(path: str) -> np.ndarray:
+    """An image file (PGM or PNG) as a 2-D uint8 array, 8-bit gray as the
+    reference's cv::imread(path, IMREAD_GRAYSCALE) reads it."""
+    w, h = _I(0), _I(0)
+    p = os.fsencode(path)
+    _check(lib().ss_read_image(p, None, 0, ctypes.byref(w), ctypes.byref(h)),
+           f"ss_read_image({path})")
+    out = np.empty((h.value, w.value), dtype=np.uint8)
+    _check(lib().ss_read_image(p, out.ctypes.data, out.size, ctypes.byref(w),
+                               ctypes.byref(h)), f"ss_read_image({path})")
+    return out
+
+
+def write_pgm(path: str, image: np.ndarray) -> None:
+    """Writes a 2-D uint8 array as a binary PGM."""
+    image = np.ascontiguousarray(image, dtype=np.uint8)
+    _check(lib().ss_write_pgm(os.fsencode(path), image.ctypes.data,
+                              image.shape[1], image.shape[0], image.shape[1]),
+           f"ss_write_pgm({path})")
 
 
 def lib() -> ctypes.CDLL:

@@ -1,8 +1,8 @@
 """Build recipe for the CUDA route library (sm_100a).
 
 Compiles ``csrc/ss_route.cu`` (the route), ``csrc/ss_server.cu`` (the
-serving loop) and ``csrc/ss_pack.cu`` (compact mask transfer, host side with
-OpenMP) into ``libsparseseam.so`` next to this file with
+serving loop), ``csrc/ss_pack.cu`` (compact mask transfer, host side with
+OpenMP) and ``csrc/ss_image_io.cpp`` (PGM / PNG files, zlib) into ``libsparseseam.so`` next to this file with
 nvcc.  The library has a plain C ABI (``include/sparse_seam.h``) and links the
 CUDA runtime statically, so it loads into any process on the GPU host, with or
 without PyTorch.
@@ -18,7 +18,8 @@ ROOT = os.path.dirname(HERE)
 INCLUDE = os.path.join(ROOT, "include")
 SOURCES = [os.path.join(HERE, "csrc", "ss_route.cu"),
            os.path.join(HERE, "csrc", "ss_server.cu"),
-           os.path.join(HERE, "csrc", "ss_pack.cu")]
+           os.path.join(HERE, "csrc", "ss_pack.cu"),
+           os.path.join(HERE, "csrc", "ss_image_io.cpp")]
 DEPENDS = SOURCES + [
     os.path.join(HERE, "csrc", name)
     for name in ("ss_device.cuh", "ss_tile.cuh", "ss_rowscan.cuh",
@@ -41,15 +42,30 @@ def command(output: str, extra=()) -> list:
         nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17",
         "-I" + INCLUDE, "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp",
         "-shared", "-Xptxas", "-warn-spills",
-        *extra, "-o", output, *SOURCES, "-lgomp",
+        *extra, "-o", output, *SOURCES, "-lgomp", "-lz",
+    ]
+
+
+HARNESS_SOURCE = os.path.join(HERE, "csrc", "ss_harness.cpp")
+HARNESS = os.path.join(HERE, "ss_harness")
+
+
+def harness_command(output: str) -> list:
+    """The command-line harness: host C++ over the C ABI, linked against
+    the library next to it (rpath $ORIGIN)."""
+    return [
+        nvcc(), *ARCH, "-O2", "-std=c++17", "-I" + INCLUDE, "-o", output,
+        HARNESS_SOURCE, "-L" + HERE, "-lsparseseam",
+        "-Xlinker", "-rpath,$ORIGIN",
     ]
 
 
 def stale() -> bool:
-    if not os.path.exists(LIBRARY):
+    if not os.path.exists(LIBRARY) or not os.path.exists(HARNESS):
         return True
-    built = os.path.getmtime(LIBRARY)
-    return any(os.path.getmtime(d) > built for d in DEPENDS)
+    built = min(os.path.getmtime(LIBRARY), os.path.getmtime(HARNESS))
+    return any(os.path.getmtime(d) > built
+               for d in DEPENDS + [HARNESS_SOURCE])
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
@@ -59,6 +75,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
     extra = ["-Xptxas", "-v"] if verbose else []
     subprocess.check_call(command(tmp, extra))
     os.replace(tmp, LIBRARY)
+    tmp = HARNESS + ".tmp"
+    subprocess.check_call(harness_command(tmp))
+    os.replace(tmp, HARNESS)
     return LIBRARY
 
 
