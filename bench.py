@@ -148,65 +148,133 @@ REASONS = [
 
 
 class ClockSampler:
+    """SM clock, power and throttle reasons sampled during a timed region.
+
+    NVML (read-only queries) is polled every ~2 ms on a thread, and only the
+    samples taken between mark_start() and mark_end() count, so even a timed
+    region of a few milliseconds gets samples of its own.  Without NVML,
+    `nvidia-smi -lms 10` is read instead (coarser).  Nothing is changed on
+    the GPU.
+    """
+
     def __init__(self, device_index: int):
         self.device_index = device_index
-        self.proc = None
-        self.lines = []
+        self.samples = []          # (t, sm_mhz, max_mhz, power_w, reasons)
+        self._stop = threading.Event()
         self._thread = None
+        self._proc = None
+        self.window = (None, None)
+        self.source = None
 
     def start(self):
-        fields = ["index", "clocks.sm", "clocks.max.sm", "power.draw"] + \
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            handle = None
+            try:
+                # The CUDA device by UUID (NVML numbers every GPU of the
+                # host, whatever CUDA_VISIBLE_DEVICES selects).
+                import torch
+                uuid = str(torch.cuda.get_device_properties(
+                    self.device_index).uuid)
+                handle = pynvml.nvmlDeviceGetHandleByUUID(
+                    uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            except Exception:
+                handle = pynvml.nvmlDeviceGetHandleByIndex(self.device_index)
+            bits = {
+                "hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown":
+                    pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown":
+                    pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap,
+            }
+            max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(
+                handle, pynvml.NVML_CLOCK_SM)
+
+            def poll():
+                while not self._stop.is_set():
+                    t = time.monotonic()
+                    try:
+                        sm = pynvml.nvmlDeviceGetClockInfo(
+                            handle, pynvml.NVML_CLOCK_SM)
+                        pw = pynvml.nvmlDeviceGetPowerUsage(handle) / 1000.0
+                        rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(
+                            handle)
+                    except Exception:
+                        break
+                    active = [n for n, b in bits.items() if rs & b]
+                    self.samples.append((t, sm, max_mhz, pw, active))
+                    time.sleep(0.002)
+            self.source = "nvml"
+            self._thread = threading.Thread(target=poll, daemon=True)
+            self._thread.start()
+            return
+        except Exception:
+            pass
+        fields = ["clocks.sm", "clocks.max.sm", "power.draw"] + \
             [q for _, q in REASONS]
         try:
-            self.proc = subprocess.Popen(
+            self._proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={','.join(fields)}",
-                 "--format=csv,noheader,nounits", "-lms", "200",
+                 "--format=csv,noheader,nounits", "-lms", "10",
                  "-i", str(self.device_index)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
-            self.proc = None
+            self._proc = None
             return
-        self._thread = threading.Thread(target=self._read, daemon=True)
+        self.source = "nvidia-smi"
+
+        def read():
+            for line in self._proc.stdout:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 3 + len(REASONS):
+                    continue
+                try:
+                    sm, mx, pw = (float(parts[0]), float(parts[1]),
+                                  float(parts[2]))
+                except ValueError:
+                    continue
+                active = [n for (n, _), v in zip(REASONS, parts[3:])
+                          if v.lower().startswith("active")]
+                self.samples.append((time.monotonic(), sm, mx, pw, active))
+        self._thread = threading.Thread(target=read, daemon=True)
         self._thread.start()
         time.sleep(0.3)
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def mark_start(self):
+        self.window = (time.monotonic(), None)
+
+    def mark_end(self):
+        self.window = (self.window[0], time.monotonic())
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
-                    "note": "nvidia-smi unavailable"}
-        time.sleep(0.25)
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+        self._stop.set()
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
         if self._thread:
             self._thread.join(timeout=2)
-        sm, smax, power = [], [], []
-        active = set()
-        for line in self.lines:
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 4 + len(REASONS):
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-                power.append(float(parts[3]))
-            except ValueError:
-                continue
-            for (name, _), val in zip(REASONS, parts[4:]):
-                if val.lower().startswith("active"):
-                    active.add(name)
-        if not sm:
+        if self.source is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
-                    "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
-                "power_w_max": max(power), "reasons": sorted(active),
-                "samples": len(sm)}
+                    "note": "neither NVML nor nvidia-smi available"}
+        t0, t1 = self.window
+        inside = [x for x in self.samples
+                  if (t0 is None or x[0] >= t0) and (t1 is None or x[0] <= t1)]
+        if not inside:
+            inside = self.samples[-1:]
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "samples": 0, "source": self.source}
+        active = sorted({r for x in inside for r in x[4]})
+        return {"sm_mhz": statistics.median(x[1] for x in inside),
+                "sm_max_mhz": max(x[2] for x in inside),
+                "power_w_max": max(x[3] for x in inside),
+                "reasons": active, "samples": len(inside),
+                "source": self.source}
 
 
 # ---------------------------------------------------------------------------
@@ -479,12 +547,14 @@ def main():
     clocks.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    clocks.mark_start()
     with torch.cuda.stream(stream):
         ev0.record(stream)
         for _ in range(args.steps):
             graph.replay()
         ev1.record(stream)
     ev1.synchronize()
+    clocks.mark_end()
     torch.cuda.synchronize()
     clock_info = clocks.stop()
     dist.barrier()
@@ -571,19 +641,21 @@ def main():
 
 def sweep(args, pkg, images, stream):
     """Batched Gpix/s of the corpus re-quantised to 256/64/16/4/2 levels at
-    T = 16 / 32 / 64 (the reference's quantisation and tile-size studies),
-    each checked against the oracle on two images."""
+    T = 16 / 32 / 64 (the reference's quantisation and tile-size studies).
+    The re-quantisation is fused into the tile load (the plan's per-image
+    gray levels), so it is inside the timed region; each setting is checked
+    against the oracle of the host-quantised image on two images."""
     import torch
     import oracle
     out = {}
     pixels = sum(im.numel() for im in images)
+    imgs = images
+    maxs = [torch.empty_like(t) for t in imgs]
+    mins = [torch.empty_like(t) for t in imgs]
     for levels in (256, 64, 16, 4, 2):
-        imgs = images if levels == 256 else [quantize_tensor(t, levels)
-                                              for t in images]
-        maxs = [torch.empty_like(t) for t in imgs]
-        mins = [torch.empty_like(t) for t in imgs]
         for tile in (16, 32, 64):
-            plan = pkg.BatchPlan(imgs, maxs, mins, tile=tile, stream=stream)
+            plan = pkg.BatchPlan(imgs, maxs, mins, tile=tile, stream=stream,
+                                 levels=levels)
             ws = plan.make_workspace(stream=stream)
             best = None
             for persistent in (False, True):
@@ -601,7 +673,7 @@ def sweep(args, pkg, images, stream):
             ws.read_status(stream)
             bad = 0
             for i in (0, len(imgs) - 1):
-                h = imgs[i].cpu().numpy()
+                h = quantize_tensor(imgs[i], levels).cpu().numpy()
                 wmx, wmn = oracle.extrema(h)
                 bad += int((maxs[i].cpu().numpy() != wmx).sum())
                 bad += int((mins[i].cpu().numpy() != wmn).sum())

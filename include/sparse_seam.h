@@ -227,6 +227,22 @@ ss_status ss_extrema_batch_pass(const void* h_plan, const void* d_plan,
                                 void* d_workspace, size_t workspace_bytes,
                                 void* stream);
 
+/* Re-quantisation fused into the tile load: the masks are those of the image
+ * re-quantised to `levels` gray levels (2..256) with the reference's rule
+ * bin = (v * levels) >> 8, v' = (bin * 255 + (levels - 1) / 2) / (levels - 1)
+ * (harness/quantization_and_scaling/gpu_common_quant_v0_7.cu:479-494, where
+ * it runs on the host before the copy); the image itself is not changed.
+ * levels 0 or 256: the image as it is.  ss_extrema_levels is ss_extrema with
+ * that option; ss_batch_plan_set_levels sets it for image `index` of a host
+ * plan (before the plan is copied to the device). */
+ss_status ss_extrema_levels(const uint8_t* d_image, int width, int height,
+                            int pitch, int tile, int levels,
+                            uint8_t* d_maxima, uint8_t* d_minima,
+                            int out_pitch, void* d_workspace,
+                            size_t workspace_bytes, void* stream);
+ss_status ss_batch_plan_set_levels(void* h_plan, size_t plan_bytes, int index,
+                                   int levels);
+
 /* Per-call launch choices: the knobs of the batch autotuner.  None of them
  * changes the masks.  No counterpart in the reference, whose tile, classify
  * threads and flatten launch are compile-time constants

@@ -192,6 +192,9 @@ SIGNATURES = {
     "ss_unpack_masks": (_I, [_VP, _VP, ctypes.c_uint64, _VP, _VP, _I]),
     "ss_enqueue_unpack_masks": (_I, [_VP, _VP, ctypes.c_uint64, _VP, _VP, _I,
                                      _VP]),
+    "ss_extrema_levels": (_I, [_VP, _I, _I, _I, _I, _I, _VP, _VP, _I, _VP,
+                               _SZ, _VP]),
+    "ss_batch_plan_set_levels": (_I, [_VP, _SZ, _I, _I]),
     "ss_read_image": (_I, [ctypes.c_char_p, _VP, _SZ, ctypes.POINTER(_I),
                            ctypes.POINTER(_I)]),
     "ss_write_pgm": (_I, [ctypes.c_char_p, _VP, _I, _I, _I]),
@@ -317,12 +320,14 @@ def _check_image_tensor(image):
 
 def extrema(image, tile: int = 32, maxima=None, minima=None,
             workspace: Optional[Workspace] = None, stream=None,
-            check: bool = False):
+            check: bool = False, levels: int = 0):
     """Regional maxima / minima masks of a device image (uint8, H x W).
 
     Enqueues the route on `stream` (torch's current stream by default) and
     returns (maxima, minima) as uint8 CUDA tensors with 0/255 values.  With
-    check=True the stream is synchronised and device errors raise.
+    check=True the stream is synchronised and device errors raise.  With
+    `levels` (2..256) the masks are those of the image re-quantised to that
+    many gray levels, done inside the tile load (ss_extrema_levels).
     """
     import torch
     h, w, pitch = _check_image_tensor(image)
@@ -338,11 +343,19 @@ def extrema(image, tile: int = 32, maxima=None, minima=None,
     if workspace is None:
         workspace = Workspace.for_image(w, h, tile, device=image.device,
                                         stream=stream)
-    st = lib().ss_extrema(image.data_ptr(), w, h, pitch, tile,
-                          maxima.data_ptr(), minima.data_ptr(),
-                          maxima.stride(0), workspace.ptr, workspace.nbytes,
-                          _stream_handle(stream))
-    _check(st, "ss_extrema")
+    if levels:
+        st = lib().ss_extrema_levels(image.data_ptr(), w, h, pitch, tile,
+                                     int(levels), maxima.data_ptr(),
+                                     minima.data_ptr(), maxima.stride(0),
+                                     workspace.ptr, workspace.nbytes,
+                                     _stream_handle(stream))
+        _check(st, "ss_extrema_levels")
+    else:
+        st = lib().ss_extrema(image.data_ptr(), w, h, pitch, tile,
+                              maxima.data_ptr(), minima.data_ptr(),
+                              maxima.stride(0), workspace.ptr,
+                              workspace.nbytes, _stream_handle(stream))
+        _check(st, "ss_extrema")
     if check:
         workspace.read_status(stream)
     return maxima, minima
@@ -358,7 +371,7 @@ class BatchPlan:
     """
 
     def __init__(self, images: Sequence, maxima: Sequence, minima: Sequence,
-                 tile: int = 32, stream=None):
+                 tile: int = 32, stream=None, levels=None):
         import torch
         if not (len(images) == len(maxima) == len(minima)):
             raise ValueError("images / maxima / minima lengths differ")
@@ -391,6 +404,15 @@ class BatchPlan:
             descs, n, tile, self.host_plan.ctypes.data, self.plan_bytes,
             ctypes.byref(ws)), "ss_batch_plan_fill")
         self.workspace_bytes = int(ws.value)
+        if levels is not None:
+            # One gray-level count for all images, or one per image.
+            per = list(levels) if hasattr(levels, "__len__") else [levels] * n
+            if len(per) != n:
+                raise ValueError("one levels value per image")
+            for i, lv in enumerate(per):
+                _check(lib().ss_batch_plan_set_levels(
+                    self.host_plan.ctypes.data, self.plan_bytes, i, int(lv)),
+                    "ss_batch_plan_set_levels")
         device = images[0].device if n else "cuda"
         self._dev = torch.empty(self.plan_bytes + 256, dtype=torch.uint8,
                                 device=device)

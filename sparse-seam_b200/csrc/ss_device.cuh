@@ -81,8 +81,23 @@ struct __align__(16) PlanImage {
     int32_t tiles_x;
     int32_t tiles_y;
     int64_t tile_base;   // global index of the image's tile (0, 0)
+    int32_t levels;      // re-quantise the pixels to this many gray levels
+                         //   as they are loaded (2..255), 0 or 256: as is
 };
 static_assert(sizeof(PlanImage) == 64, "plan entries are 64 bytes");
+
+// The reference's re-quantisation of an 8-bit value to `levels` gray levels
+// (harness/quantization_and_scaling/gpu_common_quant_v0_7.cu:479-494):
+// bin = (v * levels) >> 8, value = (bin * 255 + (levels - 1) / 2) /
+// (levels - 1).
+__host__ __device__ __forceinline__ int quantize_level(int v, int levels) {
+    const int bin = (v * levels) >> 8;
+    return (bin * 255 + (levels - 1) / 2) / (levels - 1);
+}
+
+__host__ __device__ __forceinline__ bool levels_active(int levels) {
+    return levels >= 2 && levels < 256;
+}
 
 // Device plan of a batch: header, image table, tile -> image map.
 struct __align__(16) PlanHeader {

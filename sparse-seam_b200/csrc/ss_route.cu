@@ -433,9 +433,11 @@ __global__ void init_header_kernel(Header* h) {
 // Row-scan kernels (T = 32): NW independent warps per CTA, one tile each.
 // ---------------------------------------------------------------------------
 
-// Row-scan tile pass: NW independent warps per CTA, one tile each.
+// Row-scan tile pass: NW independent warps per CTA, one tile each; at most
+// 64 registers per thread, so 32 warps fit on an SM (the shared-memory
+// limit at 6.4 KB per warp).
 template <int NW, bool kPersistent>
-__global__ void __launch_bounds__(NW * 32)
+__global__ void __launch_bounds__(NW * 32, 32 / NW)
 runs_tile_pass_kernel(Source src, Arena a) {
     __shared__ rowscan::RunSmem sm[NW];
     const int warp = static_cast<int>(threadIdx.x) >> 5;
@@ -897,10 +899,39 @@ ss_status ss_workspace_init(void* d_workspace, size_t workspace_bytes,
     return cudaGetLastError() == cudaSuccess ? SS_OK : SS_ERR_CUDA;
 }
 
+static ss_status extrema_impl(const uint8_t* d_image, int width, int height,
+                              int pitch, int tile, int levels,
+                              uint8_t* d_maxima, uint8_t* d_minima,
+                              int out_pitch, void* d_workspace,
+                              size_t workspace_bytes, void* stream);
+
 ss_status ss_extrema(const uint8_t* d_image, int width, int height, int pitch,
                      int tile, uint8_t* d_maxima, uint8_t* d_minima,
                      int out_pitch, void* d_workspace, size_t workspace_bytes,
                      void* stream) {
+    return extrema_impl(d_image, width, height, pitch, tile, 0, d_maxima,
+                        d_minima, out_pitch, d_workspace, workspace_bytes,
+                        stream);
+}
+
+ss_status ss_extrema_levels(const uint8_t* d_image, int width, int height,
+                            int pitch, int tile, int levels,
+                            uint8_t* d_maxima, uint8_t* d_minima,
+                            int out_pitch, void* d_workspace,
+                            size_t workspace_bytes, void* stream) {
+    if (levels != 0 && (levels < 2 || levels > 256)) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    return extrema_impl(d_image, width, height, pitch, tile, levels,
+                        d_maxima, d_minima, out_pitch, d_workspace,
+                        workspace_bytes, stream);
+}
+
+static ss_status extrema_impl(const uint8_t* d_image, int width, int height,
+                              int pitch, int tile, int levels,
+                              uint8_t* d_maxima, uint8_t* d_minima,
+                              int out_pitch, void* d_workspace,
+                              size_t workspace_bytes, void* stream) {
     if (!d_image || !d_maxima || !d_minima || !d_workspace || width <= 0 ||
         height <= 0 || pitch < width || out_pitch < width) {
         return SS_ERR_INVALID_VALUE;
@@ -938,6 +969,7 @@ ss_status ss_extrema(const uint8_t* d_image, int width, int height, int pitch,
     src.single.tiles_x = (width + tile - 1) / tile;
     src.single.tiles_y = (height + tile - 1) / tile;
     src.single.tile_base = 0;
+    src.single.levels = levels;
     src.total_tiles = tiles;
     return launch_route(*cfg, src, arena_at(d_workspace, L), 0,
                         static_cast<cudaStream_t>(stream));
@@ -1107,6 +1139,21 @@ ss_status ss_batch_plan_fill(const ss_image_desc* descs, int count, int tile,
     if (workspace_bytes) {
         *workspace_bytes = needed;
     }
+    return SS_OK;
+}
+
+ss_status ss_batch_plan_set_levels(void* h_plan, size_t plan_bytes, int index,
+                                   int levels) {
+    if (!h_plan || plan_bytes < sizeof(PlanHeader) ||
+        (levels != 0 && (levels < 2 || levels > 256))) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    PlanHeader* ph = static_cast<PlanHeader*>(h_plan);
+    if (ph->magic != kMagic || index < 0 || index >= ph->count ||
+        plan_bytes < plan_size(ph->count, ph->total_tiles)) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    reinterpret_cast<PlanImage*>(ph + 1)[index].levels = levels;
     return SS_OK;
 }
 

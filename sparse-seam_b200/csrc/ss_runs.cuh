@@ -184,6 +184,20 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     // Staged row r holds image row y0 - 1 + r, staged column c image column
     // x0 - 1 + c.
     {
+        // Optional re-quantisation of every loaded pixel through a 256-entry
+        // table in the (not yet used) union-find words, built before the
+        // loads so that it does not hold registers while they are in flight.
+        const bool quantise = levels_active(job.levels);
+        const uint8_t* lut = reinterpret_cast<const uint8_t*>(sm.word);
+        if (quantise) {
+            uint8_t* t8 = reinterpret_cast<uint8_t*>(sm.word);
+#pragma unroll 1
+            for (int k = 0; k < 8; ++k) {
+                const int v = k * 32 + lane;
+                t8[v] = static_cast<uint8_t>(quantize_level(v, job.levels));
+            }
+            __syncwarp();
+        }
         const int gx = g.x0 + lane;
         const bool col_ok = lane < g.tw;
         int vals[T + 2];
@@ -215,17 +229,34 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         const int hr1 = (xr < width && ok1)
                             ? static_cast<int>(__ldg(img + gy1 * pitch + xr))
                             : -1;
+        if (quantise) {
+            auto q = [&](int v) -> int16_t {
+                return static_cast<int16_t>(v >= 0 ? lut[v] : v);
+            };
 #pragma unroll
-        for (int r = 0; r < T + 2; ++r) {
-            sm.img[r * kHaloW + lane + 1] = static_cast<int16_t>(vals[r]);
+            for (int r = 0; r < T + 2; ++r) {
+                sm.img[r * kHaloW + lane + 1] = q(vals[r]);
+            }
+            sm.img[lane * kHaloW] = q(hl0);
+            sm.img[lane * kHaloW + kHaloW - 1] = q(hr0);
+            if (lane < 2) {
+                sm.img[(32 + lane) * kHaloW] = q(hl1);
+                sm.img[(32 + lane) * kHaloW + kHaloW - 1] = q(hr1);
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < T + 2; ++r) {
+                sm.img[r * kHaloW + lane + 1] = static_cast<int16_t>(vals[r]);
+            }
+            sm.img[lane * kHaloW] = static_cast<int16_t>(hl0);
+            sm.img[lane * kHaloW + kHaloW - 1] = static_cast<int16_t>(hr0);
+            if (lane < 2) {
+                sm.img[(32 + lane) * kHaloW] = static_cast<int16_t>(hl1);
+                sm.img[(32 + lane) * kHaloW + kHaloW - 1] =
+                    static_cast<int16_t>(hr1);
+            }
         }
-        sm.img[lane * kHaloW] = static_cast<int16_t>(hl0);
-        sm.img[lane * kHaloW + kHaloW - 1] = static_cast<int16_t>(hr0);
-        if (lane < 2) {
-            sm.img[(32 + lane) * kHaloW] = static_cast<int16_t>(hl1);
-            sm.img[(32 + lane) * kHaloW + kHaloW - 1] =
-                static_cast<int16_t>(hr1);
-        }
+        __syncwarp();
         uint4* w4 = reinterpret_cast<uint4*>(sm.word);
 #pragma unroll
         for (int k = 0; k < T * T / 128; ++k) {

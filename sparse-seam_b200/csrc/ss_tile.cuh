@@ -102,6 +102,8 @@ struct TileWorker {
         const int width = job.width;
         const int height = job.height;
         const int64_t pitch = job.pitch;
+        const int levels = job.levels;
+        const bool quantise = levels_active(levels);
         for (int i = static_cast<int>(threadIdx.x); i < kHalo * kHalo;
              i += NW * 32) {
             const int r = i / kHalo;
@@ -112,6 +114,9 @@ struct TileWorker {
             if (static_cast<unsigned>(gy) < static_cast<unsigned>(height) &&
                 static_cast<unsigned>(gx) < static_cast<unsigned>(width)) {
                 v = __ldg(image + gy * pitch + gx);
+                if (quantise) {
+                    v = quantize_level(v, levels);
+                }
             }
             s.img[i] = static_cast<int16_t>(v);
         }

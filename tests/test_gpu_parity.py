@@ -204,3 +204,42 @@ def test_uninitialized_workspace_is_reported():
     with pytest.raises(pkg.SparseSeamError) as e:
         pkg.extrema(img, tile=32, workspace=ws, check=True)
     assert e.value.status == 11
+
+
+@pytest.mark.parametrize("kernel_config", [(32, -2), (32, 8), (16, 4),
+                                           (64, 16)], indirect=True,
+                         ids=["rowscan", "cta32", "cta16", "cta64"])
+def test_quantisation_fused_into_the_load(kernel_config):
+    """ss_extrema_levels on the original image gives the masks of the
+    re-quantised image (the reference's rule, applied on the host there)."""
+    import importlib
+    pkg = package()
+    synth = importlib.import_module("sparse-seam_b200.synth")
+    tile = kernel_config
+    base = synth.smooth_noise(333, 517, seed=17, device="cuda")
+    host = base.cpu().numpy()
+    for levels in (2, 3, 4, 16, 64, 255, 256):
+        want = oracle.extrema(synth.quantize(host, levels))
+        mx, mn = pkg.extrema(base, tile=tile, levels=levels, check=True)
+        assert_same((mx.cpu().numpy(), mn.cpu().numpy()), want,
+                    f"levels {levels} T={tile}")
+
+
+def test_quantisation_per_image_in_a_batch():
+    import importlib
+    pkg = package()
+    synth = importlib.import_module("sparse-seam_b200.synth")
+    images = synth.uneven_batch(12, seed=4, lo=20, hi=300, device="cuda")
+    levels = [2, 4, 8, 16, 32, 64, 128, 256, 0, 3, 5, 7]
+    maxs = [torch.empty_like(i) for i in images]
+    mins = [torch.empty_like(i) for i in images]
+    for persistent in (False, True):
+        plan = pkg.BatchPlan(images, maxs, mins, tile=32, levels=levels)
+        ws = plan.make_workspace()
+        plan.run(ws, persistent=persistent)
+        ws.read_status()
+        for i, im in enumerate(images):
+            want = oracle.extrema(synth.quantize(im.cpu().numpy(),
+                                                 levels[i] or 256))
+            assert_same((maxs[i].cpu().numpy(), mins[i].cpu().numpy()), want,
+                        f"image {i} levels {levels[i]}")
