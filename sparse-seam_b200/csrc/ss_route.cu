@@ -473,74 +473,71 @@ runs_tile_pass_kernel(Source src, Arena a) {
     }
 }
 
-// Seam and resolve passes: each warp takes src.group consecutive tiles.
-template <int NW, bool kPersistent>
-__global__ void __launch_bounds__(NW * 32)
+// Passes after the row-scan tile pass: one CTA of kLaterWarps warps per
+// group of src.group consecutive tiles.
+__global__ void __launch_bounds__(rowscan::kLaterWarps * 32)
 rowscan_seam_pass_kernel(Source src, Arena a) {
-    (void)kPersistent;
     if (a.header->magic != kMagic) {
         return;
     }
     const int warp = static_cast<int>(threadIdx.x) >> 5;
-    const int64_t first =
-        (static_cast<int64_t>(blockIdx.x) * NW + warp) * src.group;
+    const int64_t first = static_cast<int64_t>(blockIdx.x) * src.group;
     if (first < src.total_tiles) {
-        rowscan::seam_pass_warp32(src, a, first);
+        rowscan::seam_pass_group(src, a, first, warp, rowscan::kLaterWarps);
     }
 }
 
-template <int NW>
-__global__ void __launch_bounds__(NW * 32)
+__global__ void __launch_bounds__(rowscan::kLaterWarps * 32)
 rowscan_flags_pass_kernel(Source src, Arena a) {
     if (a.header->magic != kMagic) {
         return;
     }
     const int warp = static_cast<int>(threadIdx.x) >> 5;
-    const int64_t first =
-        (static_cast<int64_t>(blockIdx.x) * NW + warp) * src.group;
+    const int64_t first = static_cast<int64_t>(blockIdx.x) * src.group;
     if (first < src.total_tiles) {
-        rowscan::flags_pass_warp32(src, a, first);
+        rowscan::flags_pass_group(src, a, first, warp, rowscan::kLaterWarps);
     }
 }
 
-template <int NW, bool kPersistent>
-__global__ void __launch_bounds__(NW * 32)
+template <bool kPersistent>
+__global__ void __launch_bounds__(rowscan::kLaterWarps * 32)
 rowscan_resolve_pass_kernel(Source src, Arena a) {
-    __shared__ rowscan::ResolveSmem sm[NW];
+    __shared__ rowscan::ResolveSmem sm;
+    __shared__ uint32_t next_group;
     const int warp = static_cast<int>(threadIdx.x) >> 5;
-    const int lane = static_cast<int>(threadIdx.x) & 31;
     if (a.header->magic != kMagic) {
         return;
     }
     if constexpr (kPersistent) {
         for (;;) {
-            uint32_t group = 0;
-            if (lane == 0) {
-                group = atomicAdd(&a.header->resolve_head, 1u);
+            if (threadIdx.x == 0) {
+                next_group = atomicAdd(&a.header->resolve_head, 1u);
             }
-            group = __shfl_sync(~0u, group, 0);
-            const int64_t first = static_cast<int64_t>(group) * src.group;
+            __syncthreads();
+            const int64_t first =
+                static_cast<int64_t>(next_group) * src.group;
+            __syncthreads();   // every thread has read next_group
             if (first >= src.total_tiles) {
                 break;
             }
-            rowscan::resolve_warp32(sm[warp], src, a, first);
-            __syncwarp();
+            rowscan::resolve_group(sm, src, a, first, warp,
+                                   rowscan::kLaterWarps);
         }
-        // The last warp to finish rewinds both work queues for the next call.
-        if (lane == 0) {
+        // The last CTA to finish rewinds both work queues for the next call.
+        if (threadIdx.x == 0) {
             __threadfence();
             const uint32_t done = atomicAdd(&a.header->resolve_done, 1u);
-            if (done == gridDim.x * NW - 1) {
+            if (done == gridDim.x - 1) {
                 atomicExch(&a.header->queue_head, 0u);
                 atomicExch(&a.header->resolve_head, 0u);
                 atomicExch(&a.header->resolve_done, 0u);
             }
         }
     } else {
-        const int64_t first =
-            (static_cast<int64_t>(blockIdx.x) * NW + warp) * src.group;
+        const int64_t first = static_cast<int64_t>(blockIdx.x) * src.group;
         if (first < src.total_tiles) {
-            rowscan::resolve_warp32(sm[warp], src, a, first);
+            rowscan::resolve_group(sm, src, a, first, warp,
+                                   rowscan::kLaterWarps);
         }
     }
 }
@@ -675,10 +672,9 @@ struct Config {
         32, -(NW),                                                            \
             {runs_tile_pass_kernel<NW, false>,                                \
              runs_tile_pass_kernel<NW, true>},                                \
-            {rowscan_resolve_pass_kernel<NW, false>,                          \
-             rowscan_resolve_pass_kernel<NW, true>}, NW,                      \
-            rowscan_seam_pass_kernel<NW, false>, 32 * NW,                     \
-            rowscan_flags_pass_kernel<NW>                                     \
+            {rowscan_resolve_pass_kernel<false>,                              \
+             rowscan_resolve_pass_kernel<true>}, NW,                          \
+            rowscan_seam_pass_kernel, 32, rowscan_flags_pass_kernel           \
     }
 
 static const Config kConfigs[] = {
@@ -760,13 +756,13 @@ static int sm_count() {
     return sms;
 }
 
-// Tiles per warp of the row-scan seam and resolve passes: the smallest power
-// of two (at most 32) that keeps the grid within 64 warps per SM.  Small
-// launches (one image) get one tile per warp, so each warp's chain of
-// dependent global loads is short; large batches get 32, so one warp
+// Tiles per CTA of the row-scan seam, flags and resolve passes: the smallest
+// power of two (at most 32) that keeps the grid within 8 CTAs (64 warps) per
+// SM.  Small launches (one image) get few tiles per CTA, so each chain of
+// dependent global loads is short; large batches get 32, so each warp
 // overlaps the round trips of many tiles.
 static int later_group(int64_t tiles) {
-    const int64_t target = static_cast<int64_t>(std::max(1, sm_count())) * 64;
+    const int64_t target = static_cast<int64_t>(std::max(1, sm_count())) * 8;
     int group = 1;
     while (group < 32 && tiles > static_cast<int64_t>(group) * target) {
         group *= 2;
@@ -793,12 +789,14 @@ static ss_status launch_route(const Config& cfg, const Source& src_in,
     Source src = src_in;
     const int nw = cfg.warps < 0 ? -cfg.warps : cfg.warps;
     const int threads = nw * 32;
-    // Tiles per CTA of the passes after the tile pass.
+    // Tiles per CTA of the passes after the tile pass, and their CTA size.
     int later_per_cta = cfg.later_per_cta;
+    int later_threads = threads;
     src.group = 32;
     if (cfg.seam_pass) {
         src.group = group > 0 ? group : later_group(src.total_tiles);
-        later_per_cta = src.group * nw;
+        later_per_cta = src.group;
+        later_threads = rowscan::kLaterWarps * 32;
     }
     const int p = persistent ? 1 : 0;
     const int64_t ctas1 =
@@ -809,7 +807,7 @@ static ss_status launch_route(const Config& cfg, const Source& src_in,
     unsigned grid2 = static_cast<unsigned>(ctas2);
     if (p) {
         const int g1 = persistent_grid(cfg.tile_pass[1], threads);
-        const int g2 = persistent_grid(cfg.resolve_pass[1], threads);
+        const int g2 = persistent_grid(cfg.resolve_pass[1], later_threads);
         if (g1 <= 0 || g2 <= 0) {
             return SS_ERR_CUDA;
         }
@@ -820,15 +818,15 @@ static ss_status launch_route(const Config& cfg, const Source& src_in,
         cfg.tile_pass[p]<<<grid1, threads, 0, stream>>>(src, arena);
     }
     if ((passes & 4) && cfg.seam_pass) {
-        cfg.seam_pass<<<static_cast<unsigned>(ctas2), threads, 0, stream>>>(
-            src, arena);
+        cfg.seam_pass<<<static_cast<unsigned>(ctas2), later_threads, 0,
+                        stream>>>(src, arena);
         if (cfg.flags_pass) {
-            cfg.flags_pass<<<static_cast<unsigned>(ctas2), threads, 0,
+            cfg.flags_pass<<<static_cast<unsigned>(ctas2), later_threads, 0,
                              stream>>>(src, arena);
         }
     }
     if (passes & 2) {
-        cfg.resolve_pass[p]<<<grid2, threads, 0, stream>>>(src, arena);
+        cfg.resolve_pass[p]<<<grid2, later_threads, 0, stream>>>(src, arena);
     }
     return cudaGetLastError() == cudaSuccess ? SS_OK : SS_ERR_CUDA;
 }

@@ -137,9 +137,13 @@ __device__ __forceinline__ int64_t neighbour_tile(int64_t g, int dir,
     }
 }
 
-__device__ __forceinline__ void seam_pass_warp32(const Source& src,
-                                                 const Arena& a,
-                                                 int64_t first) {
+// Passes after the tile pass: one CTA of `nwarps` warps per group of
+// `src.group` consecutive tiles (lane = tile of the group); the group's work
+// is flattened and its 32-wide steps are dealt out to the warps, so a group
+// of dense tiles is shared by all the CTA's warps.
+__device__ __forceinline__ void seam_pass_group(const Source& src,
+                                                const Arena& a, int64_t first,
+                                                int warp, int nwarps) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
     const int64_t tile = first + lane;
     const bool valid = lane < src.group && tile < src.total_tiles;
@@ -156,7 +160,7 @@ __device__ __forceinline__ void seam_pass_warp32(const Source& src,
         tiles_x = load_job(src, tile).tiles_x;
     }
     uint32_t err = 0;
-    for (uint32_t base = 0; base < total; base += 32) {
+    for (uint32_t base = 32u * warp; base < total; base += 32u * nwarps) {
         const uint32_t f = base + static_cast<uint32_t>(lane);
         const int owner = owner_of(excl, f);
         const int64_t g = first + owner;
@@ -213,9 +217,9 @@ __device__ __forceinline__ void seam_pass_warp32(const Source& src,
 // fragment ORs its flags (its zone's flags and the "decided neighbour across
 // a seam" marks of the seam pass) into its component's root.  The kernel
 // boundaries order it after every link and before every read of a root.
-__device__ __forceinline__ void flags_pass_warp32(const Source& src,
-                                                  const Arena& a,
-                                                  int64_t first) {
+__device__ __forceinline__ void flags_pass_group(const Source& src,
+                                                 const Arena& a, int64_t first,
+                                                 int warp, int nwarps) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
     const int64_t tile = first + lane;
     const bool valid = lane < src.group && tile < src.total_tiles;
@@ -226,7 +230,7 @@ __device__ __forceinline__ void flags_pass_warp32(const Source& src,
     uint32_t total = 0;
     const uint32_t excl = warp_prefix(k, total);
     uint32_t err = 0;
-    for (uint32_t base = 0; base < total; base += 32) {
+    for (uint32_t base = 32u * warp; base < total; base += 32u * nwarps) {
         const uint32_t f = base + static_cast<uint32_t>(lane);
         const int owner = owner_of(excl, f);
         const uint32_t r = f - __shfl_sync(~0u, excl, owner);
@@ -254,17 +258,24 @@ __device__ __forceinline__ uint32_t spread4(uint32_t bits) {
     return (((bits & 15u) * 0x00204081u) & 0x01010101u) * 0xFFu;
 }
 
+// Warps per CTA of the seam, flags and resolve passes.
+constexpr int kLaterWarps = 8;
+
 struct __align__(16) ResolveSmem {
-    uint8_t final_flags[32][kSlots];
+    uint8_t final_flags[32][kSlots];   // the group's fragments' verdicts
     uint8_t* maxima[32];
     uint8_t* minima[32];
     int64_t out_origin[32];   // offset of the tile's pixel (0, 0)
     int32_t out_pitch[32];
     int16_t tw[32];
     int16_t th[32];
-    uint32_t live[T];         // one tile at a time: logged pixels per row,
-    uint32_t vmax[T];         //   and those whose maxima / minima byte is 255
-    uint32_t vmin[T];
+    // Per warp, one dense tile at a time: logged pixels per row, and those
+    // whose maxima / minima byte is 255.
+    uint32_t live[kLaterWarps][T];
+    uint32_t vmax[kLaterWarps][T];
+    uint32_t vmin[kLaterWarps][T];
+    uint32_t flipped;         // tiles (bits of the group) with a verdict
+                              //   other than their tile-local one
 };
 
 // Rewrites the logged pixels of a full tile (32 x 32, rows and origins
@@ -325,9 +336,12 @@ __device__ __forceinline__ void merge_rows(uint8_t* omax, uint8_t* omin,
     }
 }
 
-__device__ __forceinline__ void resolve_warp32(ResolveSmem& sm,
-                                               const Source& src,
-                                               const Arena& a, int64_t first) {
+// Called by every warp of the CTA with the same `first`; contains
+// __syncthreads, so all of the CTA's threads must call it.
+__device__ __forceinline__ void resolve_group(ResolveSmem& sm,
+                                              const Source& src,
+                                              const Arena& a, int64_t first,
+                                              int warp, int nwarps) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
     const int64_t tile = first + lane;
     const bool valid = lane < src.group && tile < src.total_tiles;
@@ -345,7 +359,7 @@ __device__ __forceinline__ void resolve_warp32(ResolveSmem& sm,
         return;
     }
     uint32_t err = 0;
-    if (n) {
+    if (warp == 0 && n) {
         const PlanImage job = load_job(src, tile);
         const TileGeom g = tile_geom(job, tile - job.tile_base);
         sm.maxima[lane] = job.maxima;
@@ -356,9 +370,13 @@ __device__ __forceinline__ void resolve_warp32(ResolveSmem& sm,
         sm.tw[lane] = static_cast<int16_t>(g.tw);
         sm.th[lane] = static_cast<int16_t>(g.th);
     }
+    if (warp == 0 && lane == 0) {
+        sm.flipped = 0u;
+    }
+    __syncthreads();
     // Component flags of every live fragment of these tiles.
     uint32_t flipped = 0u;
-    for (uint32_t base = 0; base < total_k; base += 32) {
+    for (uint32_t base = 32u * warp; base < total_k; base += 32u * nwarps) {
         const uint32_t f = base + static_cast<uint32_t>(lane);
         const int owner = owner_of(excl_k, f);
         const uint32_t r = f - __shfl_sync(~0u, excl_k, owner);
@@ -374,14 +392,18 @@ __device__ __forceinline__ void resolve_warp32(ResolveSmem& sm,
         }
     }
     flipped = __reduce_or_sync(~0u, flipped);
-    __syncwarp();
+    if (lane == 0 && flipped) {
+        atomicOr(&sm.flipped, flipped);
+    }
+    __syncthreads();
     // Tiles with few logged runs: all of the group's runs together, their
     // bytes spread over the lanes (consecutive lanes write consecutive bytes
     // of a run).
     const uint32_t n_sparse = n <= kSparseRuns ? n : 0u;
     uint32_t total_sparse = 0u;
     const uint32_t excl_s = warp_prefix(n_sparse, total_sparse);
-    for (uint32_t base = 0; base < total_sparse; base += 32) {
+    for (uint32_t base = 32u * warp; base < total_sparse;
+         base += 32u * nwarps) {
         const uint32_t e = base + static_cast<uint32_t>(lane);
         const int owner = owner_of(excl_s, e);
         const uint32_t j = e - __shfl_sync(~0u, excl_s, owner);
@@ -423,18 +445,24 @@ __device__ __forceinline__ void resolve_warp32(ResolveSmem& sm,
             }
         }
     }
-    // Tiles with many logged runs, one at a time: their pixels and verdicts
-    // as row masks, then the tile's rows rewritten (logged bytes replaced,
-    // the others kept).
-    for (int t = 0; t < src.group; ++t) {
-        const uint32_t nt = __shfl_sync(~0u, n, t);
-        if (nt <= kSparseRuns) {
+    // Tiles with many logged runs, dealt out to the warps one tile at a
+    // time: their pixels and verdicts as row masks, then the tile's rows
+    // rewritten (logged bytes replaced, the others kept).
+    const uint32_t dense = __ballot_sync(~0u, n > kSparseRuns);
+    uint32_t* live_rows = sm.live[warp];
+    uint32_t* vmax_rows = sm.vmax[warp];
+    uint32_t* vmin_rows = sm.vmin[warp];
+    int rank = 0;
+    for (uint32_t d = dense; d; d &= d - 1u, ++rank) {
+        if (rank % nwarps != warp) {
             continue;
         }
+        const int t = __ffs(d) - 1;
+        const uint32_t nt = __shfl_sync(~0u, n, t);
         const uint32_t kt = __shfl_sync(~0u, k, t);
-        sm.live[lane] = 0u;
-        sm.vmax[lane] = 0u;
-        sm.vmin[lane] = 0u;
+        live_rows[lane] = 0u;
+        vmax_rows[lane] = 0u;
+        vmin_rows[lane] = 0u;
         __syncwarp();
         const int tw = sm.tw[t];
         const int th = sm.th[t];
@@ -451,12 +479,12 @@ __device__ __forceinline__ void resolve_warp32(ResolveSmem& sm,
             }
             const uint32_t fl = sm.final_flags[t][rec];
             const uint32_t R = ((2u << (x + n_px - 1)) - 1u) & ~((1u << x) - 1u);
-            atomicOr(&sm.live[y], R);
+            atomicOr(&live_rows[y], R);
             if (!(fl & kHasGreater)) {
-                atomicOr(&sm.vmax[y], R);
+                atomicOr(&vmax_rows[y], R);
             }
             if (!(fl & kHasSmaller)) {
-                atomicOr(&sm.vmin[y], R);
+                atomicOr(&vmin_rows[y], R);
             }
         }
         __syncwarp();
@@ -472,21 +500,24 @@ __device__ __forceinline__ void resolve_warp32(ResolveSmem& sm,
             vec = 1;
         }
         if (vec > 1) {
-            merge_rows(omax, omin, pitch, sm.live, sm.vmax, sm.vmin, vec);
+            merge_rows(omax, omin, pitch, live_rows, vmax_rows, vmin_rows,
+                       vec);
         } else {
             for (int r = 0; r < th; ++r) {
-                if ((sm.live[r] >> lane) & 1u) {
+                if ((live_rows[r] >> lane) & 1u) {
                     const int64_t o = static_cast<int64_t>(r) * pitch + lane;
-                    omax[o] = ((sm.vmax[r] >> lane) & 1u) ? 255 : 0;
-                    omin[o] = ((sm.vmin[r] >> lane) & 1u) ? 255 : 0;
+                    omax[o] = ((vmax_rows[r] >> lane) & 1u) ? 255 : 0;
+                    omin[o] = ((vmin_rows[r] >> lane) & 1u) ? 255 : 0;
                 }
             }
         }
         __syncwarp();
     }
-    if (lane == 0 && flipped) {
-        atomicAdd(&a.header->flipped_tiles, __popc(flipped));
+    if (warp == 0 && lane == 0 && sm.flipped) {
+        atomicAdd(&a.header->flipped_tiles, __popc(sm.flipped));
     }
+    // The shared arrays may be reused by the CTA's next group.
+    __syncthreads();
     if (err) {
         raise_error(a.header, err, static_cast<uint32_t>(first));
     }

@@ -294,10 +294,10 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             const unsigned hmin_n =
                 min(min(static_cast<unsigned>(Ln), static_cast<unsigned>(vn)),
                     static_cast<unsigned>(Rn));
-            const int mx = max(max(hmax_p, hmax_n), max(Lc, Rc));
-            const unsigned mn = min(min(hmin_p, hmin_n),
-                                    min(static_cast<unsigned>(Lc),
-                                        static_cast<unsigned>(Rc)));
+            // 3 x 3 maxima / minima including the centre: a neighbour is
+            // greater iff the maximum of the nine is above the centre.
+            const int mx = max(max(hmax_p, hmax_c), hmax_n);
+            const unsigned mn = min(min(hmin_p, hmin_c), hmin_n);
             const bool gt = mx > vc;
             const bool lt = mn < static_cast<unsigned>(vc);
             const bool listed = col_ok && !(gt && lt);
@@ -421,6 +421,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     __syncwarp();
 
     // -- flatten; zone flags ORed into the roots --------------------------------
+    uint32_t roots = 0u;   // run heads of this row that are zone roots
     {
         uint32_t r = heads;
         while (__any_sync(~0u, r != 0u)) {
@@ -444,6 +445,8 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                 if (root != p) {
                     // p is not a root: no other lane writes its word now.
                     vw[p] = with_parent(vw[p], p, root);
+                } else {
+                    roots |= 1u << h;
                 }
                 const uint32_t zf = (vw[root] >> kZoneShift) & 7u;
                 if ((zf & own) != own) {
@@ -457,15 +460,12 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     // -- records of live seam zones, in pixel order ----------------------------
     uint32_t live_roots = 0u;
     {
-        uint32_t r = heads;
+        uint32_t r = roots;
         while (r) {
             const int h = __ffs(r) - 1;
             r &= r - 1u;
-            const int p = run_word(y, h);
-            const uint32_t w = vw[p];
-            const uint32_t z = (w >> kZoneShift) & 7u;
-            if (rparent(w, p) == p && (z & kTouchesSeam) &&
-                (z & kDead) != kDead) {
+            const uint32_t z = (vw[run_word(y, h)] >> kZoneShift) & 7u;
+            if ((z & kTouchesSeam) && (z & kDead) != kDead) {
                 live_roots |= 1u << h;
             }
         }
@@ -592,7 +592,15 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     };
     uint32_t* items = a.seam_items + item * kSeamCap;
     int nitems = 0;
-    auto emit = [&](bool ok, uint32_t rec, int dir, int off) {
+    // Lanes are consecutive border positions.  When the previous position
+    // emits the same record in the same direction, both pairs join the same
+    // two zones (our two pixels share a record, so a zone and a value; their
+    // partners are 4-adjacent pixels of that value in one neighbour tile, so
+    // one zone there too): only the first pair of such a streak is emitted.
+    auto emit = [&](bool ok_in, uint32_t rec, int dir, int off) {
+        const int key = ok_in ? static_cast<int>(rec | (dir << 8)) : -1;
+        const int prev = __shfl_up_sync(~0u, key, 1);
+        const bool ok = ok_in && !(lane > 0 && prev == key);
         const uint32_t bal = __ballot_sync(~0u, ok);
         if (ok) {
             items[nitems + __popc(bal & lt_mask)] =
