@@ -134,28 +134,30 @@ def _time_choice(images, choice: Choice, reps: int, stream):
     return e0.elapsed_time(e1) / reps, maxs, mins
 
 
-# A candidate replaces the first (the library default) only when it is at
-# least this much faster: smaller gaps are within run-to-run noise, and equal
-# choices let TunedBatch keep the classes in one launch.
+# A class keeps its own best choice only when it beats the choice that is
+# best over all classes by at least this much: smaller gaps are within
+# run-to-run noise, and one common choice keeps the batch in one launch.
 MARGIN = 0.03
 
 
 def tune(pixels_per_class: int = 16 << 20, reps: int = 5, seed: int = 0,
          device="cuda", classes: Optional[Sequence[int]] = None,
          choices: Optional[Sequence[Choice]] = None) -> TuningTable:
-    """Times every candidate on a synthetic batch of each class and keeps the
-    fastest (the first candidate unless another beats it by MARGIN).  Raises
-    if any candidate's masks differ from the first's."""
+    """Times every candidate on a synthetic batch of each class; picks the
+    candidate fastest over all classes, and for a class its own fastest if
+    that beats the common one by MARGIN.  Raises if any candidate's masks
+    differ from the first's."""
     import torch
     stream = torch.cuda.Stream()
     cands = list(choices) if choices else candidates()
     picked: Dict[int, Choice] = {}
     timings: Dict[int, Dict[str, float]] = {}
+    raw: Dict[int, Dict[Choice, float]] = {}
     for k in (classes if classes is not None else range(len(CLASS_BOUNDS))):
         images = class_sample(k, pixels_per_class, seed + 7919 * k, device)
         ref = None
-        best = None
         timings[k] = {}
+        raw[k] = {}
         for c in cands:
             ms, mx, mn = _time_choice(images, c, reps, stream)
             if ref is None:
@@ -166,11 +168,14 @@ def tune(pixels_per_class: int = 16 << 20, reps: int = 5, seed: int = 0,
                         raise RuntimeError(
                             f"class {k}: {c.label()} changed the masks")
             timings[k][c.label()] = round(ms, 4)
-            if best is None:
-                best = (ms * (1.0 - MARGIN), c)
-            elif ms < best[0]:
-                best = (ms, c)
-        picked[k] = best[1]
+            raw[k][c] = ms
+    # One choice for every class unless a class gains more than MARGIN from
+    # its own best: every distinct choice is one more launch of the batch.
+    common = min(cands, key=lambda c: (sum(t[c] for t in raw.values()),
+                                       cands.index(c)))
+    for k, t in raw.items():
+        own = min(t, key=t.get)
+        picked[k] = own if t[own] < t[common] * (1.0 - MARGIN) else common
     return TuningTable(picked, timings)
 
 
