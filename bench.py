@@ -622,8 +622,9 @@ def main():
     if not args.quick:
         line.update(secondary(args, pkg, plan, images, host_images, maxs,
                               mins, stream, dist, hbm))
-        if not args.no_extra:
-            # Per-GPU measurements, run alike on every rank (no collective).
+        if not args.no_extra and dist.world == 1:
+            # Single-GPU workloads (the uneven-size batch, the served stream
+            # and the resolution sweep are defined on one B200).
             line["batched_uneven"] = uneven_section(args, pkg, device, stream)
             line["served"] = serving_section(args, pkg, device, stream)
             line["resolution_sweep"] = resolution_section(args, pkg, device,
@@ -745,8 +746,13 @@ def secondary(args, pkg, plan, images, host_images, maxs, mins, stream, dist,
 
     # -- e2e: host-to-host through the public API ---------------------------
     host = __import__("importlib").import_module("sparse-seam_b200.host")
+    # Every rank expands its masks on the host: the host's processors are
+    # shared among the ranks (one each left for the rank's own thread).
+    unpack_threads = 0 if dist.world == 1 else \
+        max(1, cpu_threads() // dist.world - 1)
     hb = host.HostBatch(host_images, tile=tile, chunks=8,
-                        persistent=False, packed=True, threads=0)
+                        persistent=False, packed=True,
+                        threads=unpack_threads)
     for _ in range(args.warmup):
         hb.run(stream)
     stream.synchronize()

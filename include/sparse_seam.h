@@ -357,7 +357,11 @@ typedef struct ss_server_config {
     int32_t persistent;       /* batch schedule, as in ss_extrema_batch */
     int32_t inflight;         /* batch slots, 1..16 */
     int32_t max_batch_images; /* requests per batch, >= 1 */
-    int32_t reserved;
+    int32_t unpack_threads;   /* host masks of 8 Mpixel or more with
+                               * out_pitch == width come back as bit planes
+                               * (ss_pack_masks) expanded by this many host
+                               * threads (0: half the host's processors);
+                               * -1: byte copies of every mask */
     int64_t batch_tiles;      /* tile capacity of one batch's workspace */
     uint64_t pool_bytes;      /* device bytes for request images and masks */
 } ss_server_config;

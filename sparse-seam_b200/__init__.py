@@ -127,7 +127,7 @@ class ServerConfig(ctypes.Structure):
         ("persistent", ctypes.c_int32),
         ("inflight", ctypes.c_int32),
         ("max_batch_images", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("unpack_threads", ctypes.c_int32),
         ("batch_tiles", ctypes.c_int64),
         ("pool_bytes", ctypes.c_uint64),
     ]

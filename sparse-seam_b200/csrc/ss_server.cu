@@ -9,7 +9,9 @@
 //             launched (up to the slot's image and tile capacity) becomes one
 //             batch: plan filled on the host, the slot's stream waits for the
 //             copies, the plan is copied in, the route is enqueued, then the
-//             masks are copied out and the batch's device status is read back
+//             masks come back (as bit planes expanded by host threads in a
+//             stream-ordered host function when the host masks are unpadded,
+//             else as byte copies) and the batch's device status is read back
 //             into pinned memory;
 //   complete  slots whose last event has fired hand their requests back as
 //             completions and return their pool memory;
@@ -59,6 +61,7 @@ struct Req {
     const uint8_t* d_img = nullptr;
     uint8_t* d_max = nullptr;
     uint8_t* d_min = nullptr;
+    uint32_t* d_bits = nullptr;   // compact read-back: two bit planes
     int32_t d_pitch = 0, d_out_pitch = 0;
 };
 
@@ -72,6 +75,8 @@ struct Slot {
     void* h_plan = nullptr;
     size_t plan_cap = 0;
     Header* h_header = nullptr;   // pinned copy of the status words
+    uint32_t* h_bits = nullptr;   // pinned staging of the bit planes
+    size_t bits_cap = 0;          // in 32-bit words
     std::vector<Req> reqs;
     bool busy = false;
 };
@@ -99,6 +104,8 @@ struct ss_server {
     uint64_t next_ticket = 1;              // guarded by mu
     ss_server_stats stats{};               // guarded by mu
 
+    int unpack_threads = 1;                // resolved from the config
+
     // Worker-only state.
     std::deque<Req> waiting;
     std::deque<Req> admitted;
@@ -114,13 +121,39 @@ int64_t tiles_of(int w, int h, int t) {
            static_cast<int64_t>((h + t - 1) / t);
 }
 
-size_t footprint(const ss_request& r) {
+// Pool bytes of a host request: image and two masks, plus the two bit
+// planes of the compact read-back when it applies.
+size_t plane_bytes(const ss_request& r) {
+    return ss::OffsetPool::round(static_cast<size_t>(r.width) *
+                                 static_cast<size_t>(r.height));
+}
+
+size_t bit_words(const ss_request& r) {
+    return (static_cast<size_t>(r.width) * static_cast<size_t>(r.height) +
+            31) / 32;
+}
+
+// Requests from this size on come back as bit planes: below it the byte
+// copies are shorter than the hand-off to the host function that expands
+// the planes (a few hundred microseconds).
+constexpr uint64_t kCompactMinPixels = 8ull << 20;
+
+bool compact_readback(const ss_server_config& c, const ss_request& r) {
+    return c.unpack_threads >= 0 && !(r.flags & SS_REQUEST_DEVICE) &&
+           r.out_pitch == r.width &&
+           static_cast<uint64_t>(r.width) * static_cast<uint64_t>(r.height) >=
+               kCompactMinPixels;
+}
+
+size_t footprint(const ss_server_config& c, const ss_request& r) {
     if (r.flags & SS_REQUEST_DEVICE) {
         return 0;
     }
-    const size_t plane = ss::OffsetPool::round(static_cast<size_t>(r.width) *
-                                               static_cast<size_t>(r.height));
-    return 3 * plane;
+    size_t bytes = 3 * plane_bytes(r);
+    if (compact_readback(c, r)) {
+        bytes += ss::OffsetPool::round(2 * 4 * bit_words(r));
+    }
+    return bytes;
 }
 
 void finish(ss_server* s, Slot& slot, ss_status status) {
@@ -170,12 +203,12 @@ bool admit(ss_server* s) {
             q.d_pitch = q.r.pitch;
             q.d_out_pitch = q.r.out_pitch;
         } else {
-            const size_t bytes = footprint(q.r);
+            const size_t bytes = footprint(s->cfg, q.r);
             size_t off = 0;
             if (!s->pool.alloc(bytes, &off)) {
                 break;   // the head waits for memory; arrival order is kept
             }
-            const size_t plane = bytes / 3;
+            const size_t plane = plane_bytes(q.r);
             q.pooled = true;
             q.pool_off = off;
             q.pool_bytes = bytes;
@@ -183,6 +216,9 @@ bool admit(ss_server* s) {
             q.d_img = base;
             q.d_max = base + plane;
             q.d_min = base + 2 * plane;
+            q.d_bits = compact_readback(s->cfg, q.r)
+                           ? reinterpret_cast<uint32_t*>(base + 3 * plane)
+                           : nullptr;
             q.d_pitch = q.r.width;
             q.d_out_pitch = q.r.width;
             cudaMemcpy2DAsync(base, q.r.width, q.r.image, q.r.pitch,
@@ -213,13 +249,17 @@ bool launch(ss_server* s) {
         }
         std::vector<ss_image_desc> descs;
         int64_t tiles = 0;
+        size_t words = 0;
         while (!s->admitted.empty() &&
                static_cast<int>(slot.reqs.size()) < s->cfg.max_batch_images) {
             const Req q = s->admitted.front();
-            if (tiles + q.tiles > s->cfg.batch_tiles) {
+            const size_t w = q.d_bits ? bit_words(q.r) : 0;
+            if (tiles + q.tiles > s->cfg.batch_tiles ||
+                2 * (words + w) > slot.bits_cap) {
                 break;
             }
             tiles += q.tiles;
+            words += w;
             slot.reqs.push_back(q);
             s->admitted.pop_front();
             ss_image_desc d{};
@@ -270,9 +310,29 @@ bool launch(ss_server* s) {
             st = SS_ERR_CUDA;
         }
         const int64_t t = now_ns();
+        size_t staged = 0;   // words of the slot's bit-plane staging used
         for (Req& q : slot.reqs) {
             q.launch_ns = t;
-            if (ok && !(q.r.flags & SS_REQUEST_DEVICE)) {
+            if (!ok || (q.r.flags & SS_REQUEST_DEVICE)) {
+                continue;
+            }
+            if (q.d_bits) {
+                // Compact read-back: pack on the device, copy the planes,
+                // expand them into the caller's masks on the host.
+                const uint64_t n = static_cast<uint64_t>(q.r.width) *
+                                   static_cast<uint64_t>(q.r.height);
+                const size_t w = bit_words(q.r);
+                uint32_t* hb = slot.h_bits + staged;
+                staged += 2 * w;
+                ok = ss_pack_masks(q.d_max, q.d_min, n, q.d_bits,
+                                   q.d_bits + w, slot.stream) == SS_OK &&
+                     cudaMemcpyAsync(hb, q.d_bits, 2 * 4 * w,
+                                     cudaMemcpyDeviceToHost,
+                                     slot.stream) == cudaSuccess &&
+                     ss_enqueue_unpack_masks(hb, hb + w, n, q.r.maxima,
+                                             q.r.minima, s->unpack_threads,
+                                             slot.stream) == SS_OK;
+            } else {
                 ok = cudaMemcpy2DAsync(q.r.maxima, q.r.out_pitch, q.d_max,
                                        q.d_out_pitch, q.r.width, q.r.height,
                                        cudaMemcpyDeviceToHost,
@@ -281,9 +341,9 @@ bool launch(ss_server* s) {
                                        q.d_out_pitch, q.r.width, q.r.height,
                                        cudaMemcpyDeviceToHost,
                                        slot.stream) == cudaSuccess;
-                if (!ok && st == SS_OK) {
-                    st = SS_ERR_CUDA;
-                }
+            }
+            if (!ok && st == SS_OK) {
+                st = SS_ERR_CUDA;
             }
         }
         // The batch's status words, then a clean error word for the next use.
@@ -385,6 +445,7 @@ void release_all(ss_server* s) {
         if (slot.d_plan) cudaFree(slot.d_plan);
         if (slot.h_plan) cudaFreeHost(slot.h_plan);
         if (slot.h_header) cudaFreeHost(slot.h_header);
+        if (slot.h_bits) cudaFreeHost(slot.h_bits);
     }
     s->slots.clear();
     if (s->copy_stream) {
@@ -422,7 +483,7 @@ ss_status ss_server_create(const ss_server_config* config,
     }
     if (c.device < 0 || c.inflight < 1 || c.inflight > 16 ||
         c.max_batch_images < 1 || c.max_batch_images > (1 << 20) ||
-        c.batch_tiles < 1) {
+        c.batch_tiles < 1 || c.unpack_threads < -1) {
         return SS_ERR_INVALID_VALUE;
     }
     size_t ws_bytes = 0;
@@ -437,6 +498,19 @@ ss_status ss_server_create(const ss_server_config* config,
         return SS_ERR_HOST_ALLOC;
     }
     s->cfg = c;
+    if (c.unpack_threads > 0) {
+        s->unpack_threads = c.unpack_threads;
+    } else {
+        const unsigned hw = std::thread::hardware_concurrency();
+        s->unpack_threads = hw > 3 ? static_cast<int>(hw / 2) : 1;
+    }
+    // Bit-plane staging per slot: two planes for the largest batch.
+    const size_t batch_pixels =
+        static_cast<size_t>(c.batch_tiles) * c.tile * c.tile;
+    const size_t bits_cap =
+        c.unpack_threads >= 0 ? 2 * ((batch_pixels + 31) / 32 + 32 *
+                                     static_cast<size_t>(c.max_batch_images))
+                              : 0;
     DeviceScope scope(c.device);
     bool ok = cudaStreamCreateWithFlags(&s->copy_stream,
                                         cudaStreamNonBlocking) == cudaSuccess;
@@ -449,6 +523,11 @@ ss_status ss_server_create(const ss_server_config* config,
         if (!ok) break;
         slot.ws_bytes = ws_bytes;
         slot.plan_cap = plan_cap;
+        slot.bits_cap = bits_cap;
+        if (bits_cap) {
+            ok = cudaMallocHost(reinterpret_cast<void**>(&slot.h_bits),
+                                bits_cap * 4) == cudaSuccess;
+        }
         ok = cudaStreamCreateWithFlags(&slot.stream, cudaStreamNonBlocking) ==
                  cudaSuccess &&
              cudaEventCreateWithFlags(&slot.copies_in,
@@ -491,7 +570,7 @@ ss_status ss_server_submit(ss_server* server, const ss_request* request,
     }
     const int64_t tiles = tiles_of(r.width, r.height, server->cfg.tile);
     if (tiles > server->cfg.batch_tiles ||
-        footprint(r) > server->pool.capacity()) {
+        footprint(server->cfg, r) > server->pool.capacity()) {
         return SS_ERR_TOO_LARGE;
     }
     Req q;

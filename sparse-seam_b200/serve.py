@@ -46,10 +46,10 @@ class Server:
     def __init__(self, tile: int = 32, persistent: bool = True,
                  inflight: int = 2, max_batch_images: int = 512,
                  batch_tiles: int = 1 << 16, pool_bytes: int = 1 << 30,
-                 device: int = 0):
+                 device: int = 0, unpack_threads: int = 0):
         self.config = ServerConfig(device, tile, 1 if persistent else 0,
-                                   inflight, max_batch_images, 0, batch_tiles,
-                                   pool_bytes)
+                                   inflight, max_batch_images,
+                                   unpack_threads, batch_tiles, pool_bytes)
         handle = ctypes.c_void_p()
         _pkg._check(_pkg.lib().ss_server_create(ctypes.byref(self.config),
                                                 ctypes.byref(handle)),

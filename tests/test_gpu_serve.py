@@ -33,8 +33,11 @@ def _pinned_like(t):
     return torch.empty(t.shape, dtype=torch.uint8, pin_memory=True)
 
 
-@pytest.mark.parametrize("persistent", [True, False])
-def test_mix_equals_alone_host_requests(persistent):
+@pytest.mark.parametrize("persistent,unpack", [(True, 0), (False, 3),
+                                               (True, -1)],
+                         ids=["persistent-compact", "grid-compact",
+                              "persistent-bytes"])
+def test_mix_equals_alone_host_requests(persistent, unpack):
     serve = _serve()
     images = _mixed_images(60, seed=3)
     pinned = []
@@ -45,7 +48,7 @@ def test_mix_equals_alone_host_requests(persistent):
     outs = [(_pinned_like(im), _pinned_like(im)) for im in images]
     with serve.Server(tile=32, persistent=persistent, inflight=3,
                       max_batch_images=16, batch_tiles=4096,
-                      pool_bytes=64 << 20) as srv:
+                      pool_bytes=64 << 20, unpack_threads=unpack) as srv:
         tickets = [srv.submit(pinned[i], *outs[i], user=i)
                    for i in range(len(images))]
         done = []
@@ -186,3 +189,32 @@ def test_seam_resolve_grouping_is_exact(group):
             want = oracle.extrema(im.cpu().numpy())
             assert np.array_equal(maxs[i].cpu().numpy(), want[0]), i
             assert np.array_equal(mins[i].cpu().numpy(), want[1]), i
+
+
+def test_large_requests_come_back_compact():
+    """Requests of 8 Mpixel and more take the bit-plane read-back; their
+    masks equal the oracle's like the small ones."""
+    serve = _serve()
+    synth = importlib.import_module("sparse-seam_b200.synth")
+    images = [synth.smooth_noise(2048, 4096, seed=s).cpu() for s in range(2)]
+    images.append(torch.from_numpy(synth.quantize(
+        synth.uniform_q16(2900, 2900, 5), 4)))
+    images.append(torch.from_numpy(synth.uniform_q16(300, 200, 6)))
+    pinned = []
+    for im in images:
+        p = _pinned_like(im)
+        p.copy_(im)
+        pinned.append(p)
+    outs = [(_pinned_like(im), _pinned_like(im)) for im in images]
+    with serve.Server(tile=32, inflight=2, batch_tiles=1 << 15,
+                      pool_bytes=256 << 20) as srv:
+        for i in range(len(images)):
+            srv.submit(pinned[i], *outs[i], user=i)
+        done = []
+        while len(done) < len(images):
+            done.extend(srv.poll(timeout_us=100_000))
+    assert all(c.status == 0 for c in done)
+    for i, im in enumerate(images):
+        want = oracle.extrema(im.numpy(), method="bands", threads=8)
+        assert np.array_equal(outs[i][0].numpy(), want[0]), i
+        assert np.array_equal(outs[i][1].numpy(), want[1]), i

@@ -31,7 +31,7 @@ def test_server_config_is_checked_before_any_cuda_call():
 
     def create(**kw):
         base = dict(device=0, tile=32, persistent=1, inflight=2,
-                    max_batch_images=16, reserved=0, batch_tiles=1000,
+                    max_batch_images=16, unpack_threads=0, batch_tiles=1000,
                     pool_bytes=1 << 20)
         base.update(kw)
         cfg = pkg.ServerConfig(**base)
@@ -44,6 +44,7 @@ def test_server_config_is_checked_before_any_cuda_call():
     assert create(batch_tiles=0) == 1
     assert create(device=-1) == 1
     assert create(batch_tiles=1 << 40) == 5
+    assert create(unpack_threads=-2) == 1
     assert lib.ss_server_create(None, ctypes.byref(h)) == 1
     # Calls on a null server are refused, never dereferenced.
     req = pkg.Request()
