@@ -243,3 +243,41 @@ def test_quantisation_per_image_in_a_batch():
                                                  levels[i] or 256))
             assert_same((maxs[i].cpu().numpy(), mins[i].cpu().numpy()), want,
                         f"image {i} levels {levels[i]}")
+
+
+@pytest.mark.parametrize("kernel_config", [(32, -2), (32, -4)], indirect=True,
+                         ids=["rowscan2", "rowscan4"])
+def test_every_store_width(kernel_config):
+    """Whole-row mask stores and read-merge-writes at 16, 8, 4 and 1 bytes:
+    the output pitch (and base) picks the width, the content has dense live
+    tiles (long runs across seams) and sparse ones."""
+    import importlib
+    synth = importlib.import_module("sparse-seam_b200.synth")
+    pkg = package()
+    tile = kernel_config
+    dev = torch.device("cuda")
+    rng = np.random.default_rng(77)
+    contents = {
+        "blocks": synth.blocks(257, 600, 8, 16, 3),
+        "q2": synth.quantize(synth.smooth_noise_np(257, 600, 5), 2),
+        "natural": synth.smooth_noise_np(257, 600, 6),
+        "serpentine": synth.serpentine(257, 600),
+    }
+    for name, img in contents.items():
+        want = oracle.extrema(img)
+        h, w = img.shape
+        d_img = torch.from_numpy(np.ascontiguousarray(img)).to(dev)
+        for pitch, shift in ((640, 0), (616, 0), (604, 0), (601, 0),
+                             (640, 8), (640, 4), (640, 1)):
+            base_mx = torch.full((h * pitch + 64,), 9, dtype=torch.uint8,
+                                 device=dev)
+            base_mn = torch.full((h * pitch + 64,), 9, dtype=torch.uint8,
+                                 device=dev)
+            mx = base_mx[shift:shift + h * pitch].view(h, pitch)[:, :w]
+            mn = base_mn[shift:shift + h * pitch].view(h, pitch)[:, :w]
+            pkg.extrema(d_img, tile=tile, maxima=mx, minima=mn, check=True)
+            assert_same((mx.cpu().numpy(), mn.cpu().numpy()), want,
+                        f"{name} pitch {pitch} shift {shift}")
+            # Bytes between the rows are left alone.
+            pad = base_mx[shift:shift + h * pitch].view(h, pitch)[:, w:]
+            assert (pad == 9).all(), f"{name} pitch {pitch}: wrote padding"
