@@ -750,7 +750,7 @@ def secondary(args, pkg, plan, images, host_images, maxs, mins, stream, dist,
     # shared among the ranks (one each left for the rank's own thread).
     unpack_threads = 0 if dist.world == 1 else \
         max(1, cpu_threads() // dist.world - 1)
-    hb = host.HostBatch(host_images, tile=tile, chunks=8,
+    hb = host.HostBatch(host_images, tile=tile, chunks=16,
                         persistent=False, packed=True,
                         threads=unpack_threads)
     for _ in range(args.warmup):
@@ -776,7 +776,7 @@ def secondary(args, pkg, plan, images, host_images, maxs, mins, stream, dist,
         "unit": UNIT, "h2d_bytes_per_step": hb.h2d_bytes,
         "d2h_bytes_per_step": hb.d2h_bytes,
         "ms_per_step": round(e2e_ms / args.steps, 3),
-        "api": ("sparse-seam_b200.host.HostBatch (ss_extrema_batch, 8 "
+        "api": ("sparse-seam_b200.host.HostBatch (ss_extrema_batch, 16 "
                 "chunks; masks cross the bus as bit planes and are expanded "
                 "into the pinned byte masks by all host processors but one "
                 "inside the timed region)"),

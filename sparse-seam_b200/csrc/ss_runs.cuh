@@ -125,6 +125,22 @@ __device__ __forceinline__ uint32_t range_mask(int lo, int hi) {
     return ((2u << hi) - 1u) & ~((1u << lo) - 1u);
 }
 
+// At the head h of every run, bit h of the result is set when some bit of
+// `m` lies in that run; `cont` marks the pixels that continue a run from
+// their left neighbour.  A segmented OR-scan towards the heads: before step
+// k, bit x of `link` says that pixels x .. x + 2^k - 1 each continue from
+// their left, so step k may OR in the bits 2^k further right.
+__device__ __forceinline__ uint32_t run_any(uint32_t m, uint32_t cont) {
+    uint32_t link = cont;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int sh = 1 << k;
+        m |= (m >> sh) & (link >> 1);
+        link &= (link >> sh);
+    }
+    return m;
+}
+
 // Writes the 32 x 32 mask bytes of a full tile from per-row bit masks held
 // by lane = row (`mxb`, `mnb`: 1 = byte 255), `vec` bytes per store (16, 8
 // or 4; rows and bases aligned to it).  Each store instruction covers
@@ -257,9 +273,11 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             }
         }
         __syncwarp();
+        // Words 0..255 first carry the row masks of the scan and are
+        // cleared after it.
         uint4* w4 = reinterpret_cast<uint4*>(sm.word);
 #pragma unroll
-        for (int k = 0; k < T * T / 128; ++k) {
+        for (int k = 2; k < T * T / 128; ++k) {
             w4[k * 32 + lane] = make_uint4(0u, 0u, 0u, 0u);
         }
     }
@@ -304,18 +322,17 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             const uint32_t bL = __ballot_sync(~0u, listed);
             const uint32_t bGT = __ballot_sync(~0u, listed && gt);
             const uint32_t bLT = __ballot_sync(~0u, listed && lt);
-            const uint32_t bEU = __ballot_sync(~0u, col_ok && vc == vp);
-            const uint32_t bEUL = __ballot_sync(~0u, col_ok && vc == Lp);
-            const uint32_t bEUR = __ballot_sync(~0u, col_ok && vc == Rp);
-            const uint32_t bEL = __ballot_sync(~0u, col_ok && vc == Lc);
-            if (lane == y) {
-                rL = bL;
-                rGT = bGT;
-                rLT = bLT;
-                rEU = bEU;
-                rEUL = bEUL;
-                rEUR = bEUR;
-                rEL = bEL;
+            // Equalities also at columns outside the image (-1 == -1 there):
+            // every use of these masks is restricted to listed pixels.
+            const uint32_t bEU = __ballot_sync(~0u, vc == vp);
+            const uint32_t bEUL = __ballot_sync(~0u, vc == Lp);
+            const uint32_t bEUR = __ballot_sync(~0u, vc == Rp);
+            const uint32_t bEL = __ballot_sync(~0u, vc == Lc);
+            if (lane == 0) {
+                // Row y's masks, picked up by lane y after the scan.
+                uint4* slot = reinterpret_cast<uint4*>(sm.word + 8 * y);
+                slot[0] = make_uint4(bL, bGT, bLT, bEU);
+                slot[1] = make_uint4(bEUL, bEUR, bEL, 0u);
             }
             hmax_p = hmax_c;
             hmin_p = hmin_c;
@@ -328,6 +345,26 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             Lc = Ln;
             Rc = Rn;
         }
+    }
+
+    __syncwarp();
+    {
+        // Lane y takes row y's masks (rows beyond the tile stay 0) and clears
+        // the words for the union-find.
+        uint4* slot = reinterpret_cast<uint4*>(sm.word + 8 * lane);
+        if (lane < g.th) {
+            const uint4 m0 = slot[0];
+            const uint4 m1 = slot[1];
+            rL = m0.x;
+            rGT = m0.y;
+            rLT = m0.z;
+            rEU = m0.w;
+            rEUL = m1.x;
+            rEUR = m1.y;
+            rEL = m1.z;
+        }
+        slot[0] = make_uint4(0u, 0u, 0u, 0u);
+        slot[1] = make_uint4(0u, 0u, 0u, 0u);
     }
 
     // Staged pixel (x, y) of the tile, x and y in -1 .. T.
@@ -502,7 +539,13 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     uint32_t vmax = 0u, vmin = 0u;
     int nlog = 0;
     {
-        uint32_t r = heads;
+        // Runs that hold a dead pixel, or both a pixel with a greater and
+        // one with a smaller neighbour, are in a decided zone: 0 in both
+        // masks, nothing to log; only the other runs are visited.
+        const uint32_t decided_runs =
+            run_any(dead, cont) |
+            (run_any(rGT, cont) & run_any(rLT, cont));
+        uint32_t r = heads & ~decided_runs;
         while (__any_sync(~0u, r != 0u)) {
             bool logged = false;
             uint32_t entry = 0u;
@@ -628,8 +671,9 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                             g.th == T && g.y0 + T < height;
         const int vt = px(x, 0);
         const int vb = px(x, T - 1);
+        const bool any_tb = __any_sync(~0u, live_t || live_b);
 #pragma unroll
-        for (int d = -1; d <= 1; ++d) {
+        for (int d = -1; d <= 1 && any_tb; ++d) {
             const int x2 = x + d;
             const int dir_t = x2 < 0 ? kRelTopLeft
                                      : (x2 >= T ? kRelTopRight : kRelTop);
@@ -655,8 +699,9 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                             g.tw == T && g.x0 + T < width;
         const int vl = px(0, y);
         const int vr = px(T - 1, y);
+        const bool any_lr = __any_sync(~0u, live_l || live_r);
 #pragma unroll
-        for (int d = -1; d <= 1; ++d) {
+        for (int d = -1; d <= 1 && any_lr; ++d) {
             const int y2 = y + d;
             const bool inside = y2 >= 0 && y2 < g.th;   // corners: rows above
             emit(live_l && inside && px(-1, y2) == vl, rl, kRelLeft,
