@@ -26,7 +26,10 @@
 //             above-right and not to the one above.
 // Union-find runs over run heads only, one lane per row, so its cost grows
 // with the number of runs and contacts per row rather than with the number
-// of listed pixels: a large plateau is a few runs per row.  Zone flags are
+// of listed pixels: a large plateau is a few runs per row.  Runs that no
+// union touches and no seam reaches are zones of their own: their verdicts
+// come from per-run carry tests on the row masks, and the loops over runs
+// visit only the others.  Zone flags are
 // ORed into the roots; live seam zones (touching a seam, flags not both set)
 // get records in pixel order of their roots and a log of their runs; every
 // pixel of the tile gets its mask bytes in one final pass, whole rows with
@@ -125,20 +128,40 @@ __device__ __forceinline__ uint32_t range_mask(int lo, int hi) {
     return ((2u << hi) - 1u) & ~((1u << lo) - 1u);
 }
 
-// At the head h of every run, bit h of the result is set when some bit of
-// `m` lies in that run; `cont` marks the pixels that continue a run from
-// their left neighbour.  A segmented OR-scan towards the heads: before step
-// k, bit x of `link` says that pixels x .. x + 2^k - 1 each continue from
-// their left, so step k may OR in the bits 2^k further right.
-__device__ __forceinline__ uint32_t run_any(uint32_t m, uint32_t cont) {
-    uint32_t link = cont;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        const int sh = 1 << k;
-        m |= (m >> sh) & (link >> 1);
-        link &= (link >> sh);
-    }
-    return m;
+// Per-run tests by carry propagation.  With `q` marking the pixels whose
+// right neighbour continues their run, adding a run's head bit to q sends a
+// carry through the run's pixels that stops at its end: (q + H) ^ q is the
+// whole of every run whose head is in H.  Started on q & ~m instead, the
+// carry stops at the run's first bit of m, and so reaches the run's end
+// only when no earlier pixel of the run is in m.
+struct RunShape {
+    uint32_t q;        // pixels whose right neighbour continues their run
+    uint32_t rq;       // the same in bit-reversed order (ends become heads)
+    uint32_t rheads;   // run ends, bit-reversed
+    uint32_t rends;    // run heads, bit-reversed
+};
+
+__device__ __forceinline__ RunShape run_shape(uint32_t cont, uint32_t heads,
+                                              uint32_t ends) {
+    RunShape s;
+    s.q = cont >> 1;
+    s.rq = __brev(cont);
+    s.rheads = __brev(ends);
+    s.rends = __brev(heads);
+    return s;
+}
+
+// Heads of the runs that hold no bit of m (the carry runs from each run's
+// end towards its head in bit-reversed order).
+__device__ __forceinline__ uint32_t clean_heads(const RunShape& s,
+                                                uint32_t m) {
+    const uint32_t rm = __brev(m);
+    return __brev(s.rends & ((s.rq & ~rm) + s.rheads) & ~rm);
+}
+
+// Every pixel of the runs whose heads are in hs.
+__device__ __forceinline__ uint32_t run_span(const RunShape& s, uint32_t hs) {
+    return (s.q + hs) ^ s.q;
 }
 
 // Writes the 32 x 32 mask bytes of a full tile from per-row bit masks held
@@ -426,6 +449,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
 
     // -- links: one union per contact of equal runs in rows y - 1 and y -------
     volatile uint32_t* vw = sm.word;
+    uint32_t linked = 0u;   // pixels of this row where a union touches a run
     {
         uint32_t headsm1 = __shfl_up_sync(~0u, heads, 1);
         if (y == 0) {
@@ -438,6 +462,12 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         const uint32_t B = heads & eqlUL;            // partner (x - 1, y - 1)
         const uint32_t C = ends & eqlUR & ~eqlU;     // partner (x + 1, y - 1)
         uint32_t m = A | B | C;
+        // The partners in row y - 1 of row y's contacts, handed up a lane.
+        uint32_t partners = __shfl_down_sync(~0u, A | (B >> 1) | (C << 1), 1);
+        if (y == T - 1) {
+            partners = 0u;
+        }
+        linked = m | partners;
         while (__any_sync(~0u, m != 0u)) {
             if (m) {
                 const int x = __ffs(m) - 1;
@@ -457,10 +487,28 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     }
     __syncwarp();
 
+    // -- runs that are zones of their own ---------------------------------------
+    // A run that no union touches is a whole zone; unless it touches a seam,
+    // its verdict follows from its own pixels and the flatten, record and
+    // verdict loops below leave it out (its word stays untouched; the border
+    // record of such a pixel is never asked for, since no pixel outside the
+    // tile is equal to it).  `vmax` / `vmin` start with those runs' verdicts.
+    const RunShape shape = run_shape(cont, heads, ends);
+    const uint32_t c_open = clean_heads(shape, linked | seam);
+    const uint32_t c_dead = clean_heads(shape, dead);
+    const uint32_t c_gt = clean_heads(shape, rGT);
+    const uint32_t c_lt = clean_heads(shape, rLT);
+    const uint32_t loop_heads = heads & ~c_open;
+    // Heads of runs that hold no dead pixel and not both a pixel with a
+    // greater and one with a smaller neighbour.
+    const uint32_t undecided = c_dead & (c_gt | c_lt);
+    uint32_t vmax = run_span(shape, c_open & c_dead & c_gt);
+    uint32_t vmin = run_span(shape, c_open & c_dead & c_lt);
+
     // -- flatten; zone flags ORed into the roots --------------------------------
     uint32_t roots = 0u;   // run heads of this row that are zone roots
     {
-        uint32_t r = heads;
+        uint32_t r = loop_heads;
         while (__any_sync(~0u, r != 0u)) {
             if (r) {
                 const int h = __ffs(r) - 1;
@@ -536,16 +584,12 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     // Per row (lane y): `vmax` / `vmin` hold the listed pixels of settled
     // zones whose maxima / minima byte is 255.
     uint32_t* plog = a.pending + item * kPendingCap;
-    uint32_t vmax = 0u, vmin = 0u;
     int nlog = 0;
     {
         // Runs that hold a dead pixel, or both a pixel with a greater and
         // one with a smaller neighbour, are in a decided zone: 0 in both
         // masks, nothing to log; only the other runs are visited.
-        const uint32_t decided_runs =
-            run_any(dead, cont) |
-            (run_any(rGT, cont) & run_any(rLT, cont));
-        uint32_t r = heads & ~decided_runs;
+        uint32_t r = loop_heads & undecided;
         while (__any_sync(~0u, r != 0u)) {
             bool logged = false;
             uint32_t entry = 0u;
