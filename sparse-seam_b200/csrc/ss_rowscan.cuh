@@ -68,9 +68,12 @@ struct TileGeom {
 __device__ __forceinline__ TileGeom tile_geom(const PlanImage& job,
                                               int64_t local) {
     TileGeom g;
-    const int ty = static_cast<int>(local / job.tiles_x);
-    const int tx =
-        static_cast<int>(local - static_cast<int64_t>(ty) * job.tiles_x);
+    // A 32-bit divide: a launch holds fewer than 2^31 / (4 T) tiles (its
+    // workspace refuses more, fragment ids being 32-bit).
+    const uint32_t l = static_cast<uint32_t>(local);
+    const uint32_t n = static_cast<uint32_t>(job.tiles_x);
+    const int ty = static_cast<int>(l / n);
+    const int tx = static_cast<int>(l - static_cast<uint32_t>(ty) * n);
     g.x0 = tx * T;
     g.y0 = ty * T;
     g.tw = min(T, job.width - g.x0);

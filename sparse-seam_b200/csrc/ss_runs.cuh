@@ -51,7 +51,9 @@ namespace rowscan {
 
 struct __align__(16) RunSmem {
     uint32_t word[T * T];          // union-find word at each run head
-    int16_t img[kHaloW * kHaloW];  // tile + halo, -1 outside the image
+    // Tile + halo, -1 outside the image; staged pixel (c, r) at index
+    // 1 + r * kHaloW + c, so that tile columns 4k, 4k + 1 share a word.
+    int16_t img[kHaloW * kHaloW + 2];
 };
 
 // Run-head words store the parent as (parent XOR self) in bits 0-9, so an
@@ -218,6 +220,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     const int64_t out_pitch = job.out_pitch;
     uint8_t* __restrict__ omax = job.maxima;
     uint8_t* __restrict__ omin = job.minima;
+    int16_t* const simg = sm.img + 1;
 
     // -- prologue: stage the tile and its halo; zero the words --------------
     // Staged row r holds image row y0 - 1 + r, staged column c image column
@@ -237,17 +240,8 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             }
             __syncwarp();
         }
-        const int gx = g.x0 + lane;
-        const bool col_ok = lane < g.tw;
-        int vals[T + 2];
-#pragma unroll
-        for (int r = 0; r < T + 2; ++r) {
-            const int gy = g.y0 + r - 1;
-            vals[r] = (col_ok && static_cast<unsigned>(gy) <
-                                     static_cast<unsigned>(height))
-                          ? static_cast<int>(__ldg(img + gy * pitch + gx))
-                          : -1;
-        }
+        // Halo columns x0 - 1 and x0 + T of staged rows 0..33 (lanes 0..31,
+        // then lanes 0..1 for rows 32..33).
         const int xl = g.x0 - 1;
         const int xr = g.x0 + T;
         const int gy0 = g.y0 - 1 + lane;
@@ -256,43 +250,96 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             static_cast<unsigned>(gy0) < static_cast<unsigned>(height);
         const bool ok1 = lane < 2 && static_cast<unsigned>(gy1) <
                                          static_cast<unsigned>(height);
-        const int hl0 = (xl >= 0 && ok0)
-                            ? static_cast<int>(__ldg(img + gy0 * pitch + xl))
-                            : -1;
-        const int hr0 = (xr < width && ok0)
-                            ? static_cast<int>(__ldg(img + gy0 * pitch + xr))
-                            : -1;
-        const int hl1 = (xl >= 0 && ok1)
-                            ? static_cast<int>(__ldg(img + gy1 * pitch + xl))
-                            : -1;
-        const int hr1 = (xr < width && ok1)
-                            ? static_cast<int>(__ldg(img + gy1 * pitch + xr))
-                            : -1;
-        if (quantise) {
-            auto q = [&](int v) -> int16_t {
-                return static_cast<int16_t>(v >= 0 ? lut[v] : v);
-            };
-#pragma unroll
-            for (int r = 0; r < T + 2; ++r) {
-                sm.img[r * kHaloW + lane + 1] = q(vals[r]);
-            }
-            sm.img[lane * kHaloW] = q(hl0);
-            sm.img[lane * kHaloW + kHaloW - 1] = q(hr0);
+        auto load_halo = [&](int& hl0, int& hr0, int& hl1, int& hr1) {
+            hl0 = (xl >= 0 && ok0)
+                      ? static_cast<int>(__ldg(img + gy0 * pitch + xl))
+                      : -1;
+            hr0 = (xr < width && ok0)
+                      ? static_cast<int>(__ldg(img + gy0 * pitch + xr))
+                      : -1;
+            hl1 = (xl >= 0 && ok1)
+                      ? static_cast<int>(__ldg(img + gy1 * pitch + xl))
+                      : -1;
+            hr1 = (xr < width && ok1)
+                      ? static_cast<int>(__ldg(img + gy1 * pitch + xr))
+                      : -1;
+        };
+        auto store_halo = [&](int16_t hl0, int16_t hr0, int16_t hl1,
+                              int16_t hr1) {
+            simg[lane * kHaloW] = hl0;
+            simg[lane * kHaloW + kHaloW - 1] = hr0;
             if (lane < 2) {
-                sm.img[(32 + lane) * kHaloW] = q(hl1);
-                sm.img[(32 + lane) * kHaloW + kHaloW - 1] = q(hr1);
+                simg[(32 + lane) * kHaloW] = hl1;
+                simg[(32 + lane) * kHaloW + kHaloW - 1] = hr1;
             }
+        };
+        int hl0, hr0, hl1, hr1;
+        // A tile whose halo lies inside the image, in an image whose rows
+        // start on 4-byte boundaries, is read 4 pixels per lane: 8 lanes per
+        // row, 4 rows per load instruction, each word widened to two int16
+        // pairs (tile columns 4k, 4k + 1 sit on a 4-byte boundary of the
+        // staged rows).
+        const bool word_rows =
+            !quantise && g.x0 > 0 && g.y0 > 0 && g.x0 + T < width &&
+            g.y0 + T < height &&
+            ((reinterpret_cast<uintptr_t>(img) |
+              static_cast<uintptr_t>(pitch)) & 3u) == 0;
+        if (word_rows) {
+            const int k = lane & 7;
+            const int rr = lane >> 3;
+            const uint8_t* src =
+                img + static_cast<int64_t>(g.y0 - 1 + rr) * pitch + g.x0 + 4 * k;
+            uint32_t* dst =
+                reinterpret_cast<uint32_t*>(simg + rr * kHaloW + 1 + 4 * k);
+            uint32_t w[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                w[i] = (i < 8 || rr < 2)
+                           ? __ldg(reinterpret_cast<const uint32_t*>(
+                                 src + static_cast<int64_t>(4 * i) * pitch))
+                           : 0u;
+            }
+            load_halo(hl0, hr0, hl1, hr1);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                if (i < 8 || rr < 2) {
+                    dst[i * 2 * kHaloW] = __byte_perm(w[i], 0u, 0x4140);
+                    dst[i * 2 * kHaloW + 1] = __byte_perm(w[i], 0u, 0x4342);
+                }
+            }
+            store_halo(static_cast<int16_t>(hl0), static_cast<int16_t>(hr0),
+                       static_cast<int16_t>(hl1), static_cast<int16_t>(hr1));
         } else {
+            const int gx = g.x0 + lane;
+            const bool col_ok = lane < g.tw;
+            int vals[T + 2];
 #pragma unroll
             for (int r = 0; r < T + 2; ++r) {
-                sm.img[r * kHaloW + lane + 1] = static_cast<int16_t>(vals[r]);
+                const int gy = g.y0 + r - 1;
+                vals[r] = (col_ok && static_cast<unsigned>(gy) <
+                                         static_cast<unsigned>(height))
+                              ? static_cast<int>(__ldg(img + gy * pitch + gx))
+                              : -1;
             }
-            sm.img[lane * kHaloW] = static_cast<int16_t>(hl0);
-            sm.img[lane * kHaloW + kHaloW - 1] = static_cast<int16_t>(hr0);
-            if (lane < 2) {
-                sm.img[(32 + lane) * kHaloW] = static_cast<int16_t>(hl1);
-                sm.img[(32 + lane) * kHaloW + kHaloW - 1] =
-                    static_cast<int16_t>(hr1);
+            load_halo(hl0, hr0, hl1, hr1);
+            if (quantise) {
+                auto q = [&](int v) -> int16_t {
+                    return static_cast<int16_t>(v >= 0 ? lut[v] : v);
+                };
+#pragma unroll
+                for (int r = 0; r < T + 2; ++r) {
+                    simg[r * kHaloW + lane + 1] = q(vals[r]);
+                }
+                store_halo(q(hl0), q(hr0), q(hl1), q(hr1));
+            } else {
+#pragma unroll
+                for (int r = 0; r < T + 2; ++r) {
+                    simg[r * kHaloW + lane + 1] = static_cast<int16_t>(vals[r]);
+                }
+                store_halo(static_cast<int16_t>(hl0),
+                           static_cast<int16_t>(hr0),
+                           static_cast<int16_t>(hl1),
+                           static_cast<int16_t>(hr1));
             }
         }
         __syncwarp();
@@ -310,7 +357,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     const bool col_ok = lane < g.tw;
     uint32_t rL = 0, rGT = 0, rLT = 0, rEU = 0, rEUL = 0, rEUR = 0, rEL = 0;
     {
-        const int16_t* scol = sm.img + lane;   // staged columns lane .. lane + 2
+        const int16_t* scol = simg + lane;   // staged columns lane .. lane + 2
         int Lp = scol[0];
         int vp = scol[1];
         int Rp = scol[2];
@@ -339,12 +386,10 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             // greater iff the maximum of the nine is above the centre.
             const int mx = max(max(hmax_p, hmax_c), hmax_n);
             const unsigned mn = min(min(hmin_p, hmin_c), hmin_n);
-            const bool gt = mx > vc;
-            const bool lt = mn < static_cast<unsigned>(vc);
-            const bool listed = col_ok && !(gt && lt);
-            const uint32_t bL = __ballot_sync(~0u, listed);
-            const uint32_t bGT = __ballot_sync(~0u, listed && gt);
-            const uint32_t bLT = __ballot_sync(~0u, listed && lt);
+            // Lane y derives its row's listed / greater / smaller masks from
+            // these two after the scan.
+            const uint32_t bG = __ballot_sync(~0u, mx > vc);
+            const uint32_t bS = __ballot_sync(~0u, mn < static_cast<unsigned>(vc));
             // Equalities also at columns outside the image (-1 == -1 there):
             // every use of these masks is restricted to listed pixels.
             const uint32_t bEU = __ballot_sync(~0u, vc == vp);
@@ -354,8 +399,8 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             if (lane == 0) {
                 // Row y's masks, picked up by lane y after the scan.
                 uint4* slot = reinterpret_cast<uint4*>(sm.word + 8 * y);
-                slot[0] = make_uint4(bL, bGT, bLT, bEU);
-                slot[1] = make_uint4(bEUL, bEUR, bEL, 0u);
+                slot[0] = make_uint4(bG, bS, bEU, bEUL);
+                slot[1] = make_uint4(bEUR, bEL, 0u, 0u);
             }
             hmax_p = hmax_c;
             hmin_p = hmin_c;
@@ -378,13 +423,14 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         if (lane < g.th) {
             const uint4 m0 = slot[0];
             const uint4 m1 = slot[1];
-            rL = m0.x;
-            rGT = m0.y;
-            rLT = m0.z;
-            rEU = m0.w;
-            rEUL = m1.x;
-            rEUR = m1.y;
-            rEL = m1.z;
+            const uint32_t cols = g.tw == T ? ~0u : (1u << g.tw) - 1u;
+            rL = ~(m0.x & m0.y) & cols;   // not decided, inside the image
+            rGT = rL & m0.x;
+            rLT = rL & m0.y;
+            rEU = m0.z;
+            rEUL = m0.w;
+            rEUR = m1.x;
+            rEL = m1.y;
         }
         slot[0] = make_uint4(0u, 0u, 0u, 0u);
         slot[1] = make_uint4(0u, 0u, 0u, 0u);
@@ -392,7 +438,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
 
     // Staged pixel (x, y) of the tile, x and y in -1 .. T.
     auto px = [&](int x, int y) -> int {
-        return sm.img[(y + 1) * kHaloW + x + 1];
+        return simg[(y + 1) * kHaloW + x + 1];
     };
 
     // -- seam masks: border pixels with an equal neighbour outside the tile --
