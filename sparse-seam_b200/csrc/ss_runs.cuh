@@ -125,11 +125,6 @@ __device__ __forceinline__ int head_of(uint32_t heads, int x) {
     return 31 - __clz(heads & le_mask_of(x));
 }
 
-// Bits lo..hi (0 <= lo <= hi <= 31).
-__device__ __forceinline__ uint32_t range_mask(int lo, int hi) {
-    return ((2u << hi) - 1u) & ~((1u << lo) - 1u);
-}
-
 // Per-run tests by carry propagation.  With `q` marking the pixels whose
 // right neighbour continues their run, adding a run's head bit to q sends a
 // carry through the run's pixels that stops at its end: (q + H) ^ q is the
@@ -538,7 +533,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     // its verdict follows from its own pixels and the flatten, record and
     // verdict loops below leave it out (its word stays untouched; the border
     // record of such a pixel is never asked for, since no pixel outside the
-    // tile is equal to it).  `vmax` / `vmin` start with those runs' verdicts.
+    // tile is equal to it).
     const RunShape shape = run_shape(cont, heads, ends);
     const uint32_t c_open = clean_heads(shape, linked | seam);
     const uint32_t c_dead = clean_heads(shape, dead);
@@ -548,8 +543,14 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     // Heads of runs that hold no dead pixel and not both a pixel with a
     // greater and one with a smaller neighbour.
     const uint32_t undecided = c_dead & (c_gt | c_lt);
-    uint32_t vmax = run_span(shape, c_open & c_dead & c_gt);
-    uint32_t vmin = run_span(shape, c_open & c_dead & c_lt);
+    // Each run's own zone flags at its head (a dead pixel sets both flags).
+    const uint32_t own_gt = heads & ~(c_gt & c_dead);
+    const uint32_t own_lt = heads & ~(c_lt & c_dead);
+    const uint32_t own_seam = heads & ~clean_heads(shape, seam);
+    // Heads of the runs whose maxima / minima bytes are 255; spread over the
+    // runs after the verdict loop.
+    uint32_t hmax = c_open & c_dead & c_gt;
+    uint32_t hmin = c_open & c_dead & c_lt;
 
     // -- flatten; zone flags ORed into the roots --------------------------------
     uint32_t roots = 0u;   // run heads of this row that are zone roots
@@ -559,12 +560,9 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             if (r) {
                 const int h = __ffs(r) - 1;
                 r &= r - 1u;
-                const int e = __ffs(ends & ~((1u << h) - 1u)) - 1;
-                const uint32_t R = range_mask(h, e);
-                const uint32_t own = ((rGT & R) ? kHasGreater : 0u) |
-                                     ((rLT & R) ? kHasSmaller : 0u) |
-                                     ((dead & R) ? kDead : 0u) |
-                                     ((seam & R) ? kTouchesSeam : 0u);
+                const uint32_t own = ((own_gt >> h) & 1u) * kHasGreater |
+                                     ((own_lt >> h) & 1u) * kHasSmaller |
+                                     ((own_seam >> h) & 1u) * kTouchesSeam;
                 const int p = run_word(y, h);
                 int root = p;
 #pragma unroll 1
@@ -627,8 +625,9 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     __syncwarp();
 
     // -- listed pixels: verdicts of settled zones, run log of live zones ------
-    // Per row (lane y): `vmax` / `vmin` hold the listed pixels of settled
-    // zones whose maxima / minima byte is 255.
+    // Per row (lane y): `hmax` / `hmin` collect the heads of the runs of
+    // settled zones whose maxima / minima byte is 255; `vmax` / `vmin` are
+    // those runs' pixels.
     uint32_t* plog = a.pending + item * kPendingCap;
     int nlog = 0;
     {
@@ -642,8 +641,6 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             if (r) {
                 const int h = __ffs(r) - 1;
                 r &= r - 1u;
-                const int e = __ffs(ends & ~((1u << h) - 1u)) - 1;
-                const uint32_t R = range_mask(h, e);
                 const int p = run_word(y, h);
                 const int root = rparent(vw[p], p);
                 const uint32_t w = vw[root];
@@ -652,13 +649,14 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                 if (live) {
                     const uint32_t rec1 = (w >> kRecShift) & 0xFFu;
                     if (rec1) {
+                        const int e = __ffs(ends & ~((1u << h) - 1u)) - 1;
                         logged = true;
                         entry = pending_entry(static_cast<int>(rec1 - 1u), h,
                                               y, e - h + 1);
                     }
                 } else {
-                    vmax |= (z & kHasGreater) ? 0u : R;
-                    vmin |= (z & kHasSmaller) ? 0u : R;
+                    hmax |= (z & kHasGreater) ? 0u : 1u << h;
+                    hmin |= (z & kHasSmaller) ? 0u : 1u << h;
                 }
             }
             const uint32_t bal = __ballot_sync(~0u, logged);
@@ -668,6 +666,8 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             nlog += __popc(bal);
         }
     }
+    const uint32_t vmax = run_span(shape, hmax);
+    const uint32_t vmin = run_span(shape, hmin);
     // The mask bytes of every pixel of the tile.  Pixels of live zones get a
     // placeholder 0 here and their final bytes from the resolve pass, which
     // runs after this pass; so whole rows are written, with 16-, 8- or
