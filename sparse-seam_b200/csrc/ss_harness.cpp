@@ -8,12 +8,12 @@
 //              [--device=0] [--block=16] [--warmup=5] [--reps=30]
 //              [--tile=32] [--masks]
 //
-// For every .pgm / .png file of <image_dir> (sorted by name): the image is
+// For every .pgm / .png / .bmp file of <image_dir> (sorted by name): the image is
 // read as 8-bit gray, copied to the device once, run `warmup` times, then
 // `reps` times timed with CUDA events (compute: device-resident input) and
 // `reps` times timed on the host clock from the host image to both host
 // masks (h2h: copy in, route, copy both masks out).  Masks are compared with
-// the expected masks of the same file name (PGM, or PNG), if given
+// the expected masks of the same file name (PGM, PNG or BMP), if given
 // ("oracle" columns), and with a second, independent kernel family of this
 // library (CTA-per-tile kernels at the same tile; "cross" columns).  The
 // row's memory columns count this route's device buffers: the image, both
@@ -89,10 +89,11 @@ std::vector<uint8_t> read_image(const fs::path& p, int& w, int& h) {
     return px;
 }
 
-// Expected mask of `stem` in `dir` (.pgm, else .png), or an empty vector.
+// Expected mask of `stem` in `dir` (.pgm, else .png, else .bmp), or an empty
+// vector.
 std::vector<uint8_t> expected(const fs::path& dir, const std::string& stem,
                               int w, int h) {
-    for (const char* ext : {".pgm", ".png"}) {
+    for (const char* ext : {".pgm", ".png", ".bmp"}) {
         const fs::path p = dir / (stem + ext);
         if (fs::exists(p)) {
             int ew = 0, eh = 0;
@@ -205,7 +206,8 @@ int main(int argc, char** argv) {
         std::vector<fs::path> files;
         for (const auto& e : fs::directory_iterator(image_dir)) {
             const std::string ext = e.path().extension().string();
-            if (e.is_regular_file() && (ext == ".pgm" || ext == ".png")) {
+            if (e.is_regular_file() &&
+                (ext == ".pgm" || ext == ".png" || ext == ".bmp")) {
                 files.push_back(e.path());
             }
         }

@@ -1,7 +1,9 @@
 // ss_image_io.cpp -- 8-bit grayscale image files for the harness and the
-// serving loop: PGM (P5 binary, P2 ASCII) and PNG (every colour type, bit
-// depths 1, 2, 4 and 8, all five scanline filters, not interlaced), read as
-// one byte per pixel; PGM (P5) written.
+// serving loop: PGM (P5 binary, P2 ASCII), PNG (every colour type, bit
+// depths 1, 2, 4 and 8, all five scanline filters, not interlaced) and BMP
+// (1-, 4- and 8-bit palettes, 16-bit 5-5-5 / 5-6-5, 24- and 32-bit, RLE8 and
+// RLE4, core and V1-V5 headers), read as one byte per pixel; PGM (P5)
+// written.
 //
 // The reference reads images with OpenCV, cv::imread(path,
 // IMREAD_GRAYSCALE) (harness/primary/snapshot_sparse_seam_cuda_v1_0.cu:87-103,
@@ -265,6 +267,233 @@ ss_status decode_png(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
     return SS_OK;
 }
 
+// ---- BMP -------------------------------------------------------------------
+// OpenCV's BMP decoder converts colour itself, with the weights
+// (0.114, 0.587, 0.299) for (B, G, R) held as 14-bit fractions and rounded:
+// gray = (1868 B + 9617 G + 4899 R + 8192) >> 14 (checked equal to OpenCV
+// 4.13 on 65,536 random colours).  A palette is converted entry by entry;
+// 5- and 6-bit fields are widened by a shift (no low-bit copy); pixels that
+// an RLE stream skips take palette entry 0.  32-bit pixels with bit fields
+// in a V3 or later header take a float path instead:
+// gray = (int)((0.299f R + 0.587f G) + 0.114f B) in single precision, each
+// step rounded, truncated at the end (equal to OpenCV 4.13 on all 2^24
+// colours).
+
+uint32_t le16(const uint8_t* p) {
+    return uint32_t(p[0]) | (uint32_t(p[1]) << 8);
+}
+
+uint32_t le32(const uint8_t* p) {
+    return le16(p) | (le16(p + 2) << 16);
+}
+
+uint8_t bgr_gray(int b, int g, int r) {
+    return static_cast<uint8_t>((1868 * b + 9617 * g + 4899 * r + 8192) >> 14);
+}
+
+uint8_t bgr_gray_float(int b, int g, int r) {
+    // Separate statements and volatile keep each product and sum rounded to
+    // single precision (no fused multiply-add).
+    volatile float t = 0.299f * static_cast<float>(r);
+    volatile float u = 0.587f * static_cast<float>(g);
+    t = t + u;
+    u = 0.114f * static_cast<float>(b);
+    t = t + u;
+    const int v = static_cast<int>(t);
+    return static_cast<uint8_t>(v > 255 ? 255 : v);
+}
+
+ss_status decode_bmp(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
+                     int& w, int& h) {
+    const size_t n = d.size();
+    if (n < 26 || d[0] != 'B' || d[1] != 'M') {
+        return SS_ERR_INVALID_VALUE;
+    }
+    const size_t off = le32(&d[10]);
+    const size_t hs = le32(&d[14]);
+    int64_t width = 0, height = 0;
+    uint32_t bpp = 0, comp = 0, ncolors = 0;
+    uint32_t masks[3] = {0, 0, 0};
+    size_t pal_at = 14 + hs;
+    size_t pal_entry = 4;
+    if (hs == 12) {   // OS/2 core header: 16-bit sizes, 3-byte palette
+        width = le16(&d[18]);
+        height = static_cast<int16_t>(le16(&d[20]));
+        bpp = le16(&d[24]);
+        pal_entry = 3;
+    } else if (hs >= 40 && hs <= 124 && n >= 14 + hs) {
+        width = static_cast<int32_t>(le32(&d[18]));
+        height = static_cast<int32_t>(le32(&d[22]));
+        bpp = le16(&d[28]);
+        comp = le32(&d[30]);
+        ncolors = le32(&d[46]);
+        if (comp == 3) {
+            // Bit fields: inside a V2+ header, else the 12 bytes after it.
+            size_t at = 54;
+            if (hs == 40) {
+                pal_at += 12;
+            }
+            if (n < at + 12) {
+                return SS_ERR_INVALID_VALUE;
+            }
+            for (int k = 0; k < 3; ++k) {
+                masks[k] = le32(&d[at + 4 * k]);
+            }
+        }
+    } else {
+        return SS_ERR_INVALID_VALUE;
+    }
+    const bool top_down = height < 0;
+    if (top_down) {
+        height = -height;
+    }
+    if (width <= 0 || height <= 0 || width * height > (int64_t(1) << 31)) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    // Gray value of each palette index (indices past the palette give 0).
+    uint8_t gray_pal[256] = {0};
+    if (bpp <= 8) {
+        const uint32_t cap = 1u << bpp;
+        const uint32_t count = ncolors && ncolors < cap ? ncolors : cap;
+        if (pal_at + size_t(count) * pal_entry > n) {
+            return SS_ERR_INVALID_VALUE;
+        }
+        for (uint32_t i = 0; i < count; ++i) {
+            const uint8_t* e = &d[pal_at + size_t(i) * pal_entry];
+            gray_pal[i] = bgr_gray(e[0], e[1], e[2]);
+        }
+    }
+    const size_t W = static_cast<size_t>(width);
+    const size_t H = static_cast<size_t>(height);
+    px.assign(W * H, gray_pal[0]);
+    auto row_of = [&](size_t file_row) -> uint8_t* {
+        return px.data() + (top_down ? file_row : H - 1 - file_row) * W;
+    };
+    if (comp == 1 || comp == 2) {
+        // RLE8 / RLE4: (count, index) runs; escapes 0 = end of line, 1 = end
+        // of bitmap, 2 = move by (dx, dy), n >= 3 = n literal indices padded
+        // to a 16-bit boundary.
+        const bool rle4 = comp == 2;
+        if (bpp != (rle4 ? 4u : 8u) || top_down) {
+            return SS_ERR_INVALID_VALUE;
+        }
+        size_t pos = off, x = 0, y = 0;
+        while (y < H) {
+            if (pos + 2 > n) {
+                return SS_ERR_INVALID_VALUE;
+            }
+            const uint32_t cnt = d[pos], c = d[pos + 1];
+            pos += 2;
+            if (cnt > 0) {
+                if (x + cnt > W) {
+                    return SS_ERR_INVALID_VALUE;
+                }
+                uint8_t* o = row_of(y);
+                for (uint32_t i = 0; i < cnt; ++i, ++x) {
+                    const uint32_t idx =
+                        rle4 ? ((i & 1u) ? (c & 15u) : (c >> 4)) : c;
+                    o[x] = gray_pal[idx];
+                }
+            } else if (c == 0) {
+                x = 0;
+                ++y;
+            } else if (c == 1) {
+                break;
+            } else if (c == 2) {
+                if (pos + 2 > n) {
+                    return SS_ERR_INVALID_VALUE;
+                }
+                x += d[pos];
+                y += d[pos + 1];
+                pos += 2;
+                if (x > W) {
+                    return SS_ERR_INVALID_VALUE;
+                }
+            } else {
+                const size_t bytes = rle4 ? (c + 1) / 2 : c;
+                if (x + c > W || pos + bytes > n) {
+                    return SS_ERR_INVALID_VALUE;
+                }
+                uint8_t* o = row_of(y);
+                for (uint32_t i = 0; i < c; ++i, ++x) {
+                    const uint8_t b = d[pos + (rle4 ? i / 2 : i)];
+                    const uint32_t idx =
+                        rle4 ? ((i & 1u) ? (b & 15u) : (b >> 4)) : b;
+                    o[x] = gray_pal[idx];
+                }
+                pos += (bytes + 1) & ~size_t(1);
+            }
+        }
+        w = static_cast<int>(width);
+        h = static_cast<int>(height);
+        return SS_OK;
+    }
+    // Uncompressed rows, each padded to 4 bytes.
+    // 0 palette, 1 = 555, 2 = 565, 3 = BGR, 4 = BGRx, 5 = BGRx (float)
+    int format = -1;
+    if (comp == 0) {
+        format = bpp <= 8 && (bpp == 1 || bpp == 4 || bpp == 8) ? 0
+               : bpp == 16 ? 1 : bpp == 24 ? 3 : bpp == 32 ? 4 : -1;
+    } else if (comp == 3) {
+        if (bpp == 16 && masks[0] == 0x7C00u && masks[1] == 0x03E0u &&
+            masks[2] == 0x001Fu) {
+            format = 1;
+        } else if (bpp == 16 && masks[0] == 0xF800u && masks[1] == 0x07E0u &&
+                   masks[2] == 0x001Fu) {
+            format = 2;
+        } else if (bpp == 32 && masks[0] == 0x00FF0000u &&
+                   masks[1] == 0x0000FF00u && masks[2] == 0x000000FFu) {
+            format = hs >= 56 ? 5 : 4;
+        }
+    }
+    if (format < 0) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    const size_t stride = (W * bpp + 31) / 32 * 4;
+    if (off > n || (n - off) / stride < H) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    for (size_t r = 0; r < H; ++r) {
+        const uint8_t* s = &d[off + r * stride];
+        uint8_t* o = row_of(r);
+        for (size_t x = 0; x < W; ++x) {
+            switch (format) {
+                case 0: {
+                    const size_t bit = x * bpp;
+                    const uint32_t idx =
+                        (s[bit / 8] >> (8 - bpp - bit % 8)) & ((1u << bpp) - 1u);
+                    o[x] = gray_pal[idx];
+                    break;
+                }
+                case 1: {
+                    const uint32_t t = le16(s + 2 * x);
+                    o[x] = bgr_gray((t << 3) & 0xF8, (t >> 2) & 0xF8,
+                                    (t >> 7) & 0xF8);
+                    break;
+                }
+                case 2: {
+                    const uint32_t t = le16(s + 2 * x);
+                    o[x] = bgr_gray((t << 3) & 0xF8, (t >> 3) & 0xFC,
+                                    (t >> 8) & 0xF8);
+                    break;
+                }
+                case 3:
+                    o[x] = bgr_gray(s[3 * x], s[3 * x + 1], s[3 * x + 2]);
+                    break;
+                case 4:
+                    o[x] = bgr_gray(s[4 * x], s[4 * x + 1], s[4 * x + 2]);
+                    break;
+                default:
+                    o[x] = bgr_gray_float(s[4 * x], s[4 * x + 1], s[4 * x + 2]);
+                    break;
+            }
+        }
+    }
+    w = static_cast<int>(width);
+    h = static_cast<int>(height);
+    return SS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -283,6 +512,8 @@ ss_status ss_read_image(const char* path, uint8_t* pixels, size_t capacity,
     ss_status st;
     if (data.size() >= 8 && data[0] == 137 && data[1] == 'P') {
         st = decode_png(data, px, w, h);
+    } else if (data.size() >= 2 && data[0] == 'B' && data[1] == 'M') {
+        st = decode_bmp(data, px, w, h);
     } else {
         st = decode_pgm(data, px, w, h);
     }

@@ -134,3 +134,184 @@ def test_bad_files_are_refused(tmp_path):
     notimg.write_bytes(b"\x89PNG\r\n\x1a\n" + b"\x00" * 20)
     with pytest.raises(pkg.SparseSeamError):
         pkg.read_image(str(notimg))
+
+
+# ---- BMP --------------------------------------------------------------------
+
+def write_bmp(path, pixel_rows, width, height, bpp, comp=0, palette=None,
+              masks=None, top_down=False, header=40, stream=None):
+    """A BMP file: `pixel_rows` top row first (packed bytes per row), or an
+    RLE `stream` (comp 1 / 2).  header 12 = OS/2 core, 40 = info (+ bit-field
+    masks after it), 108 / 124 = V4 / V5 (masks inside)."""
+    if stream is None:
+        stride = (width * bpp + 31) // 32 * 4
+        order = pixel_rows if top_down else pixel_rows[::-1]
+        data = b"".join(bytes(r) + b"\0" * (stride - len(r)) for r in order)
+    else:
+        data = stream
+    pal = b""
+    if palette is not None:
+        entry = 3 if header == 12 else 4
+        pal = b"".join(bytes([c[2], c[1], c[0], 0][:entry]) for c in palette)
+    if header == 12:
+        dib = struct.pack("<IHHHH", 12, width, height, 1, bpp)
+        extra = b""
+    else:
+        dib = struct.pack("<IiiHHIIiiII", header, width,
+                          -height if top_down else height, 1, bpp, comp,
+                          len(data), 2835, 2835,
+                          0 if palette is None else len(palette), 0)
+        extra = b""
+        if masks is not None and header == 40:
+            extra = struct.pack("<III", *masks)
+        if header > 40:
+            m = masks or (0, 0, 0)
+            dib += struct.pack("<IIII", m[0], m[1], m[2], 0)
+            dib += b"\0" * (header - 56)
+    off = 14 + len(dib) + len(extra) + len(pal)
+    with open(path, "wb") as f:
+        f.write(b"BM" + struct.pack("<IHHI", off + len(data), 0, 0, off) +
+                dib + extra + pal + data)
+
+
+def rle_stream(rng, width, height, rle4):
+    """A well-formed RLE8 / RLE4 stream with encoded runs, literal runs,
+    in-row moves, short rows and an end-of-bitmap mark."""
+    colors = 16 if rle4 else 256
+    out = bytearray()
+    for _ in range(height):
+        x = 0
+        stop = width if rng.random() < 0.8 else int(rng.integers(0, width + 1))
+        while x < stop:
+            left = stop - x
+            kind = rng.random()
+            if kind < 0.45 or left < 3:
+                n = int(rng.integers(1, min(255, left) + 1))
+                a, b = rng.integers(0, colors, size=2)
+                out += bytes([n, (a << 4 | b) if rle4 else a])
+            elif kind < 0.9:
+                n = int(rng.integers(3, min(255, left) + 1))
+                idx = rng.integers(0, colors, size=n)
+                if rle4:
+                    idx = np.concatenate([idx, [0]]) if n % 2 else idx
+                    lit = bytes(int(idx[i] << 4 | idx[i + 1])
+                                for i in range(0, len(idx), 2))
+                else:
+                    lit = bytes(int(v) for v in idx)
+                if len(lit) % 2:
+                    lit += b"\0"
+                out += bytes([0, n]) + lit
+            elif left > 1:
+                # A move stays inside the row (OpenCV 4.13 skips one more row
+                # after a move that ends exactly at the row's end).
+                dx = int(rng.integers(1, min(255, left - 1) + 1))
+                out += bytes([0, 2, dx, 0])
+                n = dx
+            else:
+                continue
+            x += n
+        out += bytes([0, 0])
+    out += bytes([0, 1])
+    # Bytes after the end mark are ignored; OpenCV's buffered reader wants a
+    # few there.
+    return bytes(out) + bytes(32)
+
+
+def test_bmp_matches_opencv(tmp_path):
+    cv2 = pytest.importorskip("cv2")
+    pkg = package()
+    rng = np.random.default_rng(7)
+    cases = []
+    for (h, w) in [(1, 1), (7, 13), (33, 50), (64, 3)]:
+        start = len(cases)
+        for bpp in (1, 4, 8):
+            ncol = int(rng.integers(2, (1 << bpp) + 1))
+            pal = rng.integers(0, 256, size=(ncol, 3))
+            idx = rng.integers(0, ncol, size=(h, w))
+            rows = []
+            for y in range(h):
+                bits = "".join(format(int(v), f"0{bpp}b") for v in idx[y])
+                bits += "0" * (-len(bits) % 8)
+                rows.append(bytes(int(bits[i:i + 8], 2)
+                                  for i in range(0, len(bits), 8)))
+            cases.append(dict(pixel_rows=rows, bpp=bpp, palette=pal))
+            # A core header's palette always has 2^bpp entries.
+            full = np.concatenate(
+                [pal, rng.integers(0, 256, size=((1 << bpp) - ncol, 3))])
+            cases.append(dict(pixel_rows=rows, bpp=bpp,
+                              palette=full if bpp == 8 else pal,
+                              header=12 if bpp == 8 else 40,
+                              top_down=bpp == 4))
+        v16 = rng.integers(0, 65536, size=(h, w)).astype("<u2")
+        r16 = [v16[y].tobytes() for y in range(h)]
+        cases.append(dict(pixel_rows=r16, bpp=16))
+        cases.append(dict(pixel_rows=r16, bpp=16, comp=3,
+                          masks=(0xF800, 0x07E0, 0x001F)))
+        cases.append(dict(pixel_rows=r16, bpp=16, comp=3,
+                          masks=(0x7C00, 0x03E0, 0x001F)))
+        c3 = rng.integers(0, 256, size=(h, w, 3)).astype(np.uint8)
+        r24 = [c3[y].tobytes() for y in range(h)]
+        cases.append(dict(pixel_rows=r24, bpp=24))
+        cases.append(dict(pixel_rows=r24, bpp=24, top_down=True))
+        cases.append(dict(pixel_rows=r24, bpp=24, header=12))
+        c4 = rng.integers(0, 256, size=(h, w, 4)).astype(np.uint8)
+        r32 = [c4[y].tobytes() for y in range(h)]
+        cases.append(dict(pixel_rows=r32, bpp=32))
+        cases.append(dict(pixel_rows=r32, bpp=32, comp=3, header=124,
+                          masks=(0x00FF0000, 0x0000FF00, 0x000000FF)))
+        for rle4 in (False, True):
+            ncol = 16 if rle4 else 256
+            pal = rng.integers(0, 256, size=(ncol, 3))
+            cases.append(dict(pixel_rows=None, bpp=4 if rle4 else 8,
+                              comp=2 if rle4 else 1, palette=pal,
+                              stream=rle_stream(rng, w, h, rle4)))
+        for c in cases[start:]:
+            c["size"] = (w, h)
+    for k, c in enumerate(cases):
+        w, h = c.pop("size")
+        path = str(tmp_path / f"b{k}.bmp")
+        write_bmp(path, c.pop("pixel_rows"), w, h, **c)
+        want = cv2.imread(path, cv2.IMREAD_GRAYSCALE)
+        assert want is not None, (k, c.get("bpp"), c.get("comp"))
+        got = pkg.read_image(path)
+        assert got.shape == want.shape, k
+        assert np.array_equal(got, want), (k, c.get("bpp"), c.get("comp"),
+                                           int((got != want).sum()))
+
+
+def test_bad_bmp_files_are_refused(tmp_path):
+    pkg = package()
+    good = tmp_path / "g.bmp"
+    rows = [bytes([1, 2, 3]) * 4 for _ in range(4)]
+    write_bmp(str(good), rows, 4, 4, 24)
+    data = good.read_bytes()
+    assert pkg.read_image(str(good)).shape == (4, 4)
+    cut = tmp_path / "cut.bmp"
+    cut.write_bytes(data[:-10])                  # rows missing
+    bad_bpp = tmp_path / "bpp.bmp"
+    bad_bpp.write_bytes(data[:28] + struct.pack("<H", 7) + data[30:])
+    bad_comp = tmp_path / "comp.bmp"
+    bad_comp.write_bytes(data[:30] + struct.pack("<I", 9) + data[34:])
+    run = tmp_path / "run.bmp"                  # an RLE8 run past the row
+    write_bmp(str(run), None, 4, 1, 8, comp=1, palette=[(0, 0, 0)] * 2,
+              stream=bytes([9, 1, 0, 1]))
+    for f in (cut, bad_bpp, bad_comp, run):
+        with pytest.raises(pkg.SparseSeamError):
+            pkg.read_image(str(f))
+
+
+def test_bmp_v4_bit_fields(tmp_path):
+    """16-bit bit fields inside a V4 / V5 header (which OpenCV 4.13 refuses)
+    decode as the same pixels with the fields after a 40-byte header."""
+    pkg = package()
+    rng = np.random.default_rng(9)
+    v = rng.integers(0, 65536, size=(9, 11)).astype("<u2")
+    rows = [v[y].tobytes() for y in range(9)]
+    for masks in ((0x7C00, 0x03E0, 0x001F), (0xF800, 0x07E0, 0x001F)):
+        outs = []
+        for header in (40, 108, 124):
+            path = str(tmp_path / f"v{header}.bmp")
+            write_bmp(path, rows, 11, 9, 16, comp=3, masks=masks,
+                      header=header)
+            outs.append(pkg.read_image(path))
+        assert all(np.array_equal(outs[0], o) for o in outs[1:])
