@@ -8,7 +8,8 @@
 //              [--device=0] [--block=16] [--warmup=5] [--reps=30]
 //              [--tile=32] [--masks]
 //
-// For every .pgm / .png / .bmp file of <image_dir> (sorted by name): the image is
+// For every .pgm / .png / .bmp / .jpg / .jpeg file of <image_dir> (sorted by
+// name): the image is
 // read as 8-bit gray, copied to the device once, run `warmup` times, then
 // `reps` times timed with CUDA events (compute: device-resident input) and
 // `reps` times timed on the host clock from the host image to both host
@@ -207,7 +208,8 @@ int main(int argc, char** argv) {
         for (const auto& e : fs::directory_iterator(image_dir)) {
             const std::string ext = e.path().extension().string();
             if (e.is_regular_file() &&
-                (ext == ".pgm" || ext == ".png" || ext == ".bmp")) {
+                (ext == ".pgm" || ext == ".png" || ext == ".bmp" ||
+                 ext == ".jpg" || ext == ".jpeg")) {
                 files.push_back(e.path());
             }
         }

@@ -1,9 +1,10 @@
 // ss_image_io.cpp -- 8-bit grayscale image files for the harness and the
 // serving loop: PGM (P5 binary, P2 ASCII), PNG (every colour type, bit
-// depths 1, 2, 4 and 8, all five scanline filters, not interlaced) and BMP
+// depths 1, 2, 4 and 8, all five scanline filters, not interlaced), BMP
 // (1-, 4- and 8-bit palettes, 16-bit 5-5-5 / 5-6-5, 24- and 32-bit, RLE8 and
-// RLE4, core and V1-V5 headers), read as one byte per pixel; PGM (P5)
-// written.
+// RLE4, core and V1-V5 headers) and JPEG (baseline / extended sequential
+// Huffman, 8-bit, gray or YCbCr, any sampling, restart intervals, EXIF
+// orientation), read as one byte per pixel; PGM (P5) written.
 //
 // The reference reads images with OpenCV, cv::imread(path,
 // IMREAD_GRAYSCALE) (harness/primary/snapshot_sparse_seam_cuda_v1_0.cu:87-103,
@@ -17,6 +18,7 @@
 // restated here with zlib for the decompression.
 #include <zlib.h>
 
+#include <algorithm>
 #include <cctype>
 #include <cstdint>
 #include <cstdio>
@@ -494,6 +496,577 @@ ss_status decode_bmp(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
     return SS_OK;
 }
 
+// ---- JPEG ------------------------------------------------------------------
+// Baseline and extended sequential Huffman JPEG, 8-bit samples.  OpenCV asks
+// its JPEG library for gray output, which for a YCbCr (or one-component)
+// file is the luma plane itself: the Y blocks are entropy-decoded,
+// dequantised and inverse-transformed, the chroma blocks only decoded to
+// keep the bit stream in step.  The inverse DCT is the Loeffler-Ligtenberg-
+// Moschytz factorisation in the fixed point of the IJG "islow" method:
+// constants x 2^13, two extra fraction bits between the column and the row
+// pass, rounding shifts, and the output offset by 128 and limited through a
+// 10-bit wrap-around table.  The EXIF orientation tag is applied as imread
+// applies it.  Progressive, lossless, arithmetic-coded and 12-bit files,
+// and colour spaces other than YCbCr / gray, are refused.
+
+struct JpegHuff {
+    int maxcode[18];
+    int valptr[17];
+    int mincode[17];
+    uint8_t vals[256];
+    bool defined = false;
+};
+
+bool build_huff(const uint8_t* counts, const uint8_t* vals, int nvals,
+                JpegHuff& h) {
+    int code = 0, k = 0;
+    for (int len = 1; len <= 16; ++len) {
+        h.valptr[len] = k;
+        h.mincode[len] = code;
+        code += counts[len - 1];
+        k += counts[len - 1];
+        h.maxcode[len] = counts[len - 1] ? code - 1 : -1;
+        if (code > (1 << len)) {
+            return false;
+        }
+        code <<= 1;
+    }
+    h.maxcode[17] = 0x7FFFFFFF;
+    if (k != nvals || k > 256) {
+        return false;
+    }
+    std::memcpy(h.vals, vals, static_cast<size_t>(k));
+    h.defined = true;
+    return true;
+}
+
+// Entropy-coded data: 0xFF 0x00 is a data byte 0xFF; any other 0xFF xx is a
+// marker, after which the reader returns zero bits and `short_data` records
+// that a bit past the segment was used (the file is then refused).
+struct JpegBits {
+    const uint8_t* d;
+    size_t n;
+    size_t pos;
+    uint32_t acc = 0;
+    int cnt = 0;
+    int real = 0;   // bits of `acc` that came from the segment
+    bool at_marker = false;
+    bool short_data = false;
+
+    void take(int k) {
+        if (k > real) {
+            short_data = true;
+            real = 0;
+        } else {
+            real -= k;
+        }
+    }
+
+    void fill() {
+        while (cnt <= 24) {
+            uint32_t b = 0;
+            if (pos >= n) {
+                at_marker = true;   // the file ends inside the segment
+            }
+            if (!at_marker) {
+                b = d[pos];
+                if (b == 0xFF) {
+                    const uint32_t next = pos + 1 < n ? d[pos + 1] : 0xD9;
+                    if (next == 0x00) {
+                        pos += 2;
+                    } else {
+                        at_marker = true;
+                        b = 0;
+                    }
+                } else {
+                    ++pos;
+                }
+            }
+            acc |= b << (24 - cnt);
+            if (!at_marker) {
+                real += 8;
+            }
+            cnt += 8;
+        }
+    }
+    int bits(int k) {
+        if (k == 0) {
+            return 0;
+        }
+        fill();
+        const int v = static_cast<int>(acc >> (32 - k));
+        acc <<= k;
+        cnt -= k;
+        take(k);
+        return v;
+    }
+    int decode(const JpegHuff& h) {
+        fill();
+        int code = 0;
+        for (int len = 1; len <= 16; ++len) {
+            code = (code << 1) | static_cast<int>(acc >> 31);
+            acc <<= 1;
+            --cnt;
+            take(1);
+            if (code <= h.maxcode[len]) {
+                return h.vals[h.valptr[len] + code - h.mincode[len]];
+            }
+        }
+        return -1;
+    }
+    // Skips to the byte after the next RSTn marker (restart interval end).
+    bool restart() {
+        acc = 0;
+        cnt = 0;
+        real = 0;
+        at_marker = false;
+        while (pos + 1 < n) {
+            if (d[pos] == 0xFF && d[pos + 1] >= 0xD0 && d[pos + 1] <= 0xD7) {
+                pos += 2;
+                return true;
+            }
+            if (d[pos] == 0xFF && d[pos + 1] != 0x00 && d[pos + 1] != 0xFF) {
+                return false;
+            }
+            ++pos;
+        }
+        return false;
+    }
+};
+
+int extend(int v, int t) {
+    return v < (1 << (t - 1)) ? v - (1 << t) + 1 : v;
+}
+
+const uint8_t kZigzag[64] = {
+    0,  1,  8,  16, 9,  2,  3,  10, 17, 24, 32, 25, 18, 11, 4,  5,
+    12, 19, 26, 33, 40, 48, 41, 34, 27, 20, 13, 6,  7,  14, 21, 28,
+    35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23, 30, 37, 44, 51,
+    58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63};
+
+// Output sample of a row-pass value: + 128, limited to 0..255 through a
+// 10-bit wrap (values beyond +-512 wrap as the IJG table does).
+uint8_t idct_limit(int64_t x) {
+    const int v = static_cast<int>(x & 1023);
+    if (v < 128) return static_cast<uint8_t>(v + 128);
+    if (v < 512) return 255;
+    if (v < 896) return 0;
+    return static_cast<uint8_t>(v - 896);
+}
+
+// 8 x 8 inverse DCT of dequantised coefficients (natural order) into
+// `out` (row stride `stride`).
+void idct_islow(const int32_t* in, uint8_t* out, size_t stride) {
+    // sqrt(2) times cosine combinations (c_k = cos(k pi / 16)), x 2^13:
+    constexpr int64_t k0_298 = 2446;    // -c1 + c3 + c5 - c7
+    constexpr int64_t k0_390 = 3196;    // c3 - c5
+    constexpr int64_t k0_541 = 4433;    // c6
+    constexpr int64_t k0_765 = 6270;    // c2 - c6
+    constexpr int64_t k0_899 = 7373;    // c3 - c7
+    constexpr int64_t k1_175 = 9633;    // c3
+    constexpr int64_t k1_501 = 12299;   // c1 + c3 - c5 - c7
+    constexpr int64_t k1_847 = 15137;   // c2 + c6
+    constexpr int64_t k1_961 = 16069;   // c3 + c5
+    constexpr int64_t k2_053 = 16819;   // c1 + c3 - c5 + c7
+    constexpr int64_t k2_562 = 20995;   // c1 + c3
+    constexpr int64_t k3_072 = 25172;   // c1 + c3 + c5 - c7
+    constexpr int kConst = 13, kPass1 = 2;
+    auto descale = [](int64_t x, int nb) -> int64_t {
+        return (x + (int64_t(1) << (nb - 1))) >> nb;
+    };
+    // One 8-point transform: x[0..7] in, y[0..7] before the final shift.
+    auto butterfly = [&](const int64_t* x, int64_t* y) {
+        int64_t z2 = x[2], z3 = x[6];
+        int64_t z1 = (z2 + z3) * k0_541;
+        const int64_t t2 = z1 - z3 * k1_847;
+        const int64_t t3 = z1 + z2 * k0_765;
+        const int64_t t0 = (x[0] + x[4]) << kConst;
+        const int64_t t1 = (x[0] - x[4]) << kConst;
+        const int64_t t10 = t0 + t3, t13 = t0 - t3;
+        const int64_t t11 = t1 + t2, t12 = t1 - t2;
+        int64_t o0 = x[7], o1 = x[5], o2 = x[3], o3 = x[1];
+        z1 = o0 + o3;
+        z2 = o1 + o2;
+        z3 = o0 + o2;
+        int64_t z4 = o1 + o3;
+        const int64_t z5 = (z3 + z4) * k1_175;
+        o0 *= k0_298;
+        o1 *= k2_053;
+        o2 *= k3_072;
+        o3 *= k1_501;
+        z1 *= -k0_899;
+        z2 *= -k2_562;
+        z3 = z3 * -k1_961 + z5;
+        z4 = z4 * -k0_390 + z5;
+        o0 += z1 + z3;
+        o1 += z2 + z4;
+        o2 += z2 + z3;
+        o3 += z1 + z4;
+        y[0] = t10 + o3;
+        y[7] = t10 - o3;
+        y[1] = t11 + o2;
+        y[6] = t11 - o2;
+        y[2] = t12 + o1;
+        y[5] = t12 - o1;
+        y[3] = t13 + o0;
+        y[4] = t13 - o0;
+    };
+    int64_t ws[64];
+    for (int c = 0; c < 8; ++c) {   // columns
+        int64_t x[8], y[8];
+        for (int r = 0; r < 8; ++r) {
+            x[r] = in[r * 8 + c];
+        }
+        butterfly(x, y);
+        for (int r = 0; r < 8; ++r) {
+            ws[r * 8 + c] = descale(y[r], kConst - kPass1);
+        }
+    }
+    for (int r = 0; r < 8; ++r) {   // rows
+        int64_t y[8];
+        butterfly(ws + r * 8, y);
+        for (int c = 0; c < 8; ++c) {
+            out[r * stride + c] =
+                idct_limit(descale(y[c], kConst + kPass1 + 3));
+        }
+    }
+}
+
+// EXIF orientation (tag 0x0112 of IFD0) from an APP1 payload, 1 if none.
+int exif_orientation(const uint8_t* p, size_t len) {
+    if (len < 14 || std::memcmp(p, "Exif\0\0", 6) != 0) {
+        return 1;
+    }
+    const uint8_t* t = p + 6;
+    const size_t tn = len - 6;
+    const bool le = t[0] == 'I' && t[1] == 'I';
+    if (!le && !(t[0] == 'M' && t[1] == 'M')) {
+        return 1;
+    }
+    auto u16 = [&](size_t at) -> uint32_t {
+        return le ? uint32_t(t[at]) | (uint32_t(t[at + 1]) << 8)
+                  : (uint32_t(t[at]) << 8) | uint32_t(t[at + 1]);
+    };
+    auto u32 = [&](size_t at) -> uint32_t {
+        return le ? u16(at) | (u16(at + 2) << 16)
+                  : (u16(at) << 16) | u16(at + 2);
+    };
+    const size_t ifd = u32(4);
+    if (ifd + 2 > tn) {
+        return 1;
+    }
+    const uint32_t count = u16(ifd);
+    for (uint32_t i = 0; i < count; ++i) {
+        const size_t e = ifd + 2 + size_t(i) * 12;
+        if (e + 12 > tn) {
+            break;
+        }
+        if (u16(e) == 0x0112 && u16(e + 2) == 3) {
+            const uint32_t v = u16(e + 8);
+            return v >= 1 && v <= 8 ? static_cast<int>(v) : 1;
+        }
+    }
+    return 1;
+}
+
+// Applies EXIF orientation o to a w x h image (w, h updated).
+void orient(std::vector<uint8_t>& px, int& w, int& h, int o) {
+    if (o <= 1) {
+        return;
+    }
+    const bool swap = o >= 5;
+    const int nw = swap ? h : w, nh = swap ? w : h;
+    std::vector<uint8_t> out(px.size());
+    for (int y = 0; y < nh; ++y) {
+        for (int x = 0; x < nw; ++x) {
+            int sx, sy;   // source pixel of output (x, y)
+            switch (o) {
+                case 2: sx = w - 1 - x; sy = y; break;
+                case 3: sx = w - 1 - x; sy = h - 1 - y; break;
+                case 4: sx = x; sy = h - 1 - y; break;
+                case 5: sx = y; sy = x; break;
+                case 6: sx = y; sy = h - 1 - x; break;
+                case 7: sx = w - 1 - y; sy = h - 1 - x; break;
+                default: sx = w - 1 - y; sy = x; break;   // 8
+            }
+            out[size_t(y) * nw + x] = px[size_t(sy) * w + sx];
+        }
+    }
+    px.swap(out);
+    w = nw;
+    h = nh;
+}
+
+ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
+                      int& w, int& h) {
+    const size_t n = d.size();
+    if (n < 4 || d[0] != 0xFF || d[1] != 0xD8) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    uint16_t qt[4][64];
+    bool qt_defined[4] = {false, false, false, false};
+    JpegHuff dc[4], ac[4];
+    struct Comp {
+        int id, hs, vs, tq;
+    } comps[4];
+    int ncomp = 0, width = 0, height = 0, restart = 0, orientation = 1;
+    bool adobe_rgb = false;
+    std::vector<uint8_t> plane;
+    size_t plane_w = 0;
+    int y_blocks_w = 0, y_blocks_h = 0, hmax = 1, vmax = 1;
+    bool y_done = false;
+    size_t pos = 2;
+    while (pos + 4 <= n) {
+        if (d[pos] != 0xFF) {
+            ++pos;   // stray bytes between segments
+            continue;
+        }
+        const uint8_t m = d[pos + 1];
+        if (m == 0xFF) {
+            ++pos;
+            continue;
+        }
+        pos += 2;
+        if (m == 0xD9) {
+            break;   // end of image
+        }
+        if ((m >= 0xD0 && m <= 0xD7) || m == 0x01) {
+            continue;
+        }
+        const size_t len = (size_t(d[pos]) << 8) | d[pos + 1];
+        if (len < 2 || pos + len > n) {
+            return SS_ERR_INVALID_VALUE;
+        }
+        const uint8_t* seg = &d[pos + 2];
+        const size_t sl = len - 2;
+        if (m == 0xE1) {
+            if (orientation == 1) {
+                orientation = exif_orientation(seg, sl);
+            }
+        } else if (m == 0xEE) {
+            // Adobe: transform 0 with three components means RGB samples.
+            if (sl >= 12 && std::memcmp(seg, "Adobe", 5) == 0 && seg[11] == 0) {
+                adobe_rgb = true;
+            }
+        } else if (m == 0xDB) {
+            size_t q = 0;
+            while (q < sl) {
+                const int pq = seg[q] >> 4, tq = seg[q] & 15;
+                if (tq > 3 || pq > 1 || q + 1 + 64 * (pq + 1) > sl) {
+                    return SS_ERR_INVALID_VALUE;
+                }
+                for (int k = 0; k < 64; ++k) {
+                    qt[tq][kZigzag[k]] = static_cast<uint16_t>(
+                        pq ? (seg[q + 1 + 2 * k] << 8) | seg[q + 2 + 2 * k]
+                           : seg[q + 1 + k]);
+                }
+                qt_defined[tq] = true;
+                q += 1 + 64 * (pq + 1);
+            }
+        } else if (m == 0xC4) {
+            size_t q = 0;
+            while (q + 17 <= sl) {
+                const int tc = seg[q] >> 4, th = seg[q] & 15;
+                int total = 0;
+                for (int k = 0; k < 16; ++k) {
+                    total += seg[q + 1 + k];
+                }
+                if (tc > 1 || th > 3 || q + 17 + total > sl ||
+                    !build_huff(seg + q + 1, seg + q + 17, total,
+                                tc ? ac[th] : dc[th])) {
+                    return SS_ERR_INVALID_VALUE;
+                }
+                q += 17 + total;
+            }
+        } else if (m == 0xDD) {
+            if (sl < 2) {
+                return SS_ERR_INVALID_VALUE;
+            }
+            restart = (seg[0] << 8) | seg[1];
+        } else if (m == 0xC0 || m == 0xC1) {
+            if (sl < 6 || seg[0] != 8) {
+                return SS_ERR_INVALID_VALUE;
+            }
+            height = (seg[1] << 8) | seg[2];
+            width = (seg[3] << 8) | seg[4];
+            ncomp = seg[5];
+            if (width <= 0 || height <= 0 || (ncomp != 1 && ncomp != 3) ||
+                sl < 6 + size_t(3) * ncomp) {
+                return SS_ERR_INVALID_VALUE;   // DNL heights, CMYK refused
+            }
+            for (int i = 0; i < ncomp; ++i) {
+                comps[i].id = seg[6 + 3 * i];
+                comps[i].hs = seg[7 + 3 * i] >> 4;
+                comps[i].vs = seg[7 + 3 * i] & 15;
+                comps[i].tq = seg[8 + 3 * i];
+                if (comps[i].hs < 1 || comps[i].hs > 4 || comps[i].vs < 1 ||
+                    comps[i].vs > 4 || comps[i].tq > 3) {
+                    return SS_ERR_INVALID_VALUE;
+                }
+                hmax = std::max(hmax, comps[i].hs);
+                vmax = std::max(vmax, comps[i].vs);
+            }
+            // Gray output is the first component at full resolution.
+            if (comps[0].hs != hmax || comps[0].vs != vmax ||
+                (ncomp == 3 && comps[0].id == 'R' && comps[1].id == 'G' &&
+                 comps[2].id == 'B')) {
+                return SS_ERR_INVALID_VALUE;
+            }
+            const int mcu_w = 8 * hmax, mcu_h = 8 * vmax;
+            const int mcus_x = (width + mcu_w - 1) / mcu_w;
+            const int mcus_y = (height + mcu_h - 1) / mcu_h;
+            y_blocks_w = mcus_x * hmax;
+            y_blocks_h = mcus_y * vmax;
+            plane_w = size_t(y_blocks_w) * 8;
+            plane.assign(plane_w * size_t(y_blocks_h) * 8, 0);
+        } else if ((m >= 0xC2 && m <= 0xCF) && m != 0xC4 && m != 0xC8 &&
+                   m != 0xCC) {
+            return SS_ERR_INVALID_VALUE;   // progressive, lossless, arithmetic
+        } else if (m == 0xDA) {
+            if (plane.empty() || sl < 1) {
+                return SS_ERR_INVALID_VALUE;
+            }
+            const int ns = seg[0];
+            if (ns < 1 || ns > ncomp || sl < 4 + size_t(2) * ns) {
+                return SS_ERR_INVALID_VALUE;
+            }
+            int sc[4], std_dc[4], std_ac[4];
+            bool has_y = false;
+            for (int i = 0; i < ns; ++i) {
+                const int cid = seg[1 + 2 * i];
+                sc[i] = -1;
+                for (int k = 0; k < ncomp; ++k) {
+                    if (comps[k].id == cid) sc[i] = k;
+                }
+                std_dc[i] = seg[2 + 2 * i] >> 4;
+                std_ac[i] = seg[2 + 2 * i] & 15;
+                if (sc[i] < 0 || std_dc[i] > 3 || std_ac[i] > 3) {
+                    return SS_ERR_INVALID_VALUE;
+                }
+                has_y = has_y || sc[i] == 0;
+            }
+            const uint8_t ss = seg[1 + 2 * ns], se = seg[2 + 2 * ns],
+                          a = seg[3 + 2 * ns];
+            if (ss != 0 || se != 63 || a != 0) {
+                return SS_ERR_INVALID_VALUE;
+            }
+            pos += len;
+            if (!has_y) {
+                // Chroma only: skip the entropy-coded data.
+                while (pos + 1 < n && !(d[pos] == 0xFF && d[pos + 1] != 0x00 &&
+                                        !(d[pos + 1] >= 0xD0 && d[pos + 1] <= 0xD7))) {
+                    ++pos;
+                }
+                continue;
+            }
+            for (int i = 0; i < ns; ++i) {
+                const int k = sc[i];
+                if (!dc[std_dc[i]].defined || !ac[std_ac[i]].defined ||
+                    !qt_defined[comps[k].tq]) {
+                    return SS_ERR_INVALID_VALUE;
+                }
+            }
+            JpegBits br{d.data(), n, pos};
+            int pred[4] = {0, 0, 0, 0};
+            // Units: interleaved MCUs, or the blocks of the one component.
+            int units_x, units_y;
+            if (ns > 1) {
+                units_x = (width + 8 * hmax - 1) / (8 * hmax);
+                units_y = (height + 8 * vmax - 1) / (8 * vmax);
+            } else {
+                const int cw = (width * comps[sc[0]].hs + hmax - 1) / hmax;
+                const int ch = (height * comps[sc[0]].vs + vmax - 1) / vmax;
+                units_x = (cw + 7) / 8;
+                units_y = (ch + 7) / 8;
+            }
+            int32_t coef[64];
+            int64_t unit = 0;
+            for (int uy = 0; uy < units_y; ++uy) {
+                for (int ux = 0; ux < units_x; ++ux, ++unit) {
+                    if (restart && unit > 0 && unit % restart == 0) {
+                        if (br.short_data || !br.restart()) {
+                            return SS_ERR_INVALID_VALUE;
+                        }
+                        pred[0] = pred[1] = pred[2] = pred[3] = 0;
+                    }
+                    for (int i = 0; i < ns; ++i) {
+                        const int k = sc[i];
+                        const int bh = ns > 1 ? comps[k].hs : 1;
+                        const int bv = ns > 1 ? comps[k].vs : 1;
+                        for (int by = 0; by < bv; ++by) {
+                            for (int bx = 0; bx < bh; ++bx) {
+                                std::memset(coef, 0, sizeof(coef));
+                                const int t = br.decode(dc[std_dc[i]]);
+                                if (t < 0 || t > 11) {
+                                    return SS_ERR_INVALID_VALUE;
+                                }
+                                pred[i] += t ? extend(br.bits(t), t) : 0;
+                                const uint16_t* q = qt[comps[k].tq];
+                                coef[0] = pred[i] * q[0];
+                                for (int z = 1; z < 64;) {
+                                    const int rs = br.decode(ac[std_ac[i]]);
+                                    if (rs < 0) {
+                                        return SS_ERR_INVALID_VALUE;
+                                    }
+                                    const int r = rs >> 4, sz = rs & 15;
+                                    if (sz == 0) {
+                                        if (r != 15) break;   // end of block
+                                        z += 16;
+                                        continue;
+                                    }
+                                    z += r;
+                                    if (z > 63) {
+                                        return SS_ERR_INVALID_VALUE;
+                                    }
+                                    const int nat = kZigzag[z];
+                                    coef[nat] = extend(br.bits(sz), sz) * q[nat];
+                                    ++z;
+                                }
+                                if (k != 0) {
+                                    continue;
+                                }
+                                const int gx = ns > 1 ? ux * hmax + bx : ux;
+                                const int gy = ns > 1 ? uy * vmax + by : uy;
+                                if (gx < y_blocks_w && gy < y_blocks_h) {
+                                    idct_islow(coef,
+                                               plane.data() + size_t(gy) * 8 *
+                                                                  plane_w +
+                                                   size_t(gx) * 8,
+                                               plane_w);
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            if (br.short_data) {
+                return SS_ERR_INVALID_VALUE;   // the data ended too early
+            }
+            y_done = true;
+            // Continue after the entropy-coded segment.
+            pos = br.pos;
+            while (pos + 1 < n && !(d[pos] == 0xFF && d[pos + 1] != 0x00 &&
+                                    !(d[pos + 1] >= 0xD0 && d[pos + 1] <= 0xD7))) {
+                ++pos;
+            }
+            continue;
+        }
+        pos += len;
+    }
+    if (!y_done || (ncomp == 3 && adobe_rgb)) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    px.resize(size_t(width) * height);
+    for (int y = 0; y < height; ++y) {
+        std::memcpy(px.data() + size_t(y) * width, plane.data() + size_t(y) * plane_w,
+                    size_t(width));
+    }
+    w = width;
+    h = height;
+    orient(px, w, h, orientation);
+    return SS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -514,6 +1087,8 @@ ss_status ss_read_image(const char* path, uint8_t* pixels, size_t capacity,
         st = decode_png(data, px, w, h);
     } else if (data.size() >= 2 && data[0] == 'B' && data[1] == 'M') {
         st = decode_bmp(data, px, w, h);
+    } else if (data.size() >= 2 && data[0] == 0xFF && data[1] == 0xD8) {
+        st = decode_jpeg(data, px, w, h);
     } else {
         st = decode_pgm(data, px, w, h);
     }

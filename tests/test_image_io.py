@@ -315,3 +315,90 @@ def test_bmp_v4_bit_fields(tmp_path):
                       header=header)
             outs.append(pkg.read_image(path))
         assert all(np.array_equal(outs[0], o) for o in outs[1:])
+
+
+# ---- JPEG -------------------------------------------------------------------
+
+JPEG_PARAMS = [
+    ("q95", "IMWRITE_JPEG_QUALITY", 95),
+    ("q20", "IMWRITE_JPEG_QUALITY", 20),
+    ("q100", "IMWRITE_JPEG_QUALITY", 100),
+    ("444", "IMWRITE_JPEG_SAMPLING_FACTOR", "IMWRITE_JPEG_SAMPLING_FACTOR_444"),
+    ("422", "IMWRITE_JPEG_SAMPLING_FACTOR", "IMWRITE_JPEG_SAMPLING_FACTOR_422"),
+    ("411", "IMWRITE_JPEG_SAMPLING_FACTOR", "IMWRITE_JPEG_SAMPLING_FACTOR_411"),
+    ("restart3", "IMWRITE_JPEG_RST_INTERVAL", 3),
+    ("optimised", "IMWRITE_JPEG_OPTIMIZE", 1),
+]
+
+
+def _jpeg_inputs(rng):
+    for (h, w) in [(1, 1), (7, 13), (33, 50), (64, 3), (17, 16), (321, 481)]:
+        noise = rng.integers(0, 256, size=(h, w, 3)).astype(np.uint8)
+        yy, xx = np.mgrid[0:h, 0:w]
+        smooth = np.stack([(xx * 5 + yy * 3) % 256, (xx * 2 + yy * 7) % 256,
+                           (xx * 11) % 256], -1).astype(np.uint8)
+        yield noise
+        yield smooth
+        yield noise[..., 0].copy()   # one-component file
+
+
+@pytest.mark.parametrize("name,key,value", JPEG_PARAMS,
+                         ids=[p[0] for p in JPEG_PARAMS])
+def test_jpeg_matches_opencv(tmp_path, name, key, value):
+    cv2 = pytest.importorskip("cv2")
+    pkg = package()
+    rng = np.random.default_rng(11)
+    if isinstance(value, str):
+        value = getattr(cv2, value)
+    for k, img in enumerate(_jpeg_inputs(rng)):
+        ok, buf = cv2.imencode(".jpg", img, [getattr(cv2, key), value])
+        assert ok
+        path = str(tmp_path / f"{name}_{k}.jpg")
+        with open(path, "wb") as f:
+            f.write(buf.tobytes())
+        want = cv2.imread(path, cv2.IMREAD_GRAYSCALE)
+        got = pkg.read_image(path)
+        assert got.shape == want.shape, (name, k)
+        assert np.array_equal(got, want), (name, k, int((got != want).sum()))
+
+
+def test_jpeg_exif_orientation(tmp_path):
+    cv2 = pytest.importorskip("cv2")
+    pkg = package()
+    rng = np.random.default_rng(12)
+    img = rng.integers(0, 256, size=(13, 21, 3)).astype(np.uint8)
+    ok, buf = cv2.imencode(".jpg", img, [cv2.IMWRITE_JPEG_QUALITY, 90])
+    base = buf.tobytes()
+    for little in (True, False):
+        e = "<" if little else ">"
+        for o in range(1, 9):
+            tiff = ((b"II" if little else b"MM") + struct.pack(e + "HI", 42, 8)
+                    + struct.pack(e + "H", 1)
+                    + struct.pack(e + "HHIHH", 0x0112, 3, 1, o, 0)
+                    + struct.pack(e + "I", 0))
+            payload = b"Exif\0\0" + tiff
+            app1 = b"\xff\xe1" + struct.pack(">H", len(payload) + 2) + payload
+            path = str(tmp_path / f"o{o}{int(little)}.jpg")
+            with open(path, "wb") as f:
+                f.write(base[:2] + app1 + base[2:])
+            want = cv2.imread(path, cv2.IMREAD_GRAYSCALE)
+            got = pkg.read_image(path)
+            assert got.shape == want.shape, (o, little)
+            assert np.array_equal(got, want), (o, little)
+
+
+def test_jpeg_refusals(tmp_path):
+    cv2 = pytest.importorskip("cv2")
+    pkg = package()
+    rng = np.random.default_rng(13)
+    img = rng.integers(0, 256, size=(40, 40, 3)).astype(np.uint8)
+    ok, prog = cv2.imencode(".jpg", img, [cv2.IMWRITE_JPEG_PROGRESSIVE, 1])
+    ok, base = cv2.imencode(".jpg", img)
+    files = {"progressive": prog.tobytes(),
+             "truncated": base.tobytes()[:len(base) // 2],
+             "no_frame": b"\xff\xd8\xff\xd9"}
+    for name, data in files.items():
+        p = tmp_path / f"{name}.jpg"
+        p.write_bytes(data)
+        with pytest.raises(pkg.SparseSeamError):
+            pkg.read_image(str(p))
