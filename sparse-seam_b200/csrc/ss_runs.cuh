@@ -31,7 +31,8 @@
 // come from per-run carry tests on the row masks, and the loops over runs
 // visit only the others.  Zone flags are
 // ORed into the roots; live seam zones (touching a seam, flags not both set)
-// get records in pixel order of their roots and a log of their runs; every
+// get records (numbered as the verdict loop first meets them) and a log of
+// their runs; every
 // pixel of the tile gets its mask bytes in one final pass, whole rows with
 // vector stores where the output allows (live pixels get a placeholder that
 // the resolve pass replaces); border records and seam items go to the
@@ -553,7 +554,6 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     uint32_t hmin = c_open & c_dead & c_lt;
 
     // -- flatten; zone flags ORed into the roots --------------------------------
-    uint32_t roots = 0u;   // run heads of this row that are zone roots
     {
         uint32_t r = loop_heads;
         while (__any_sync(~0u, r != 0u)) {
@@ -574,8 +574,6 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                 if (root != p) {
                     // p is not a root: no other lane writes its word now.
                     vw[p] = with_parent(vw[p], p, root);
-                } else {
-                    roots |= 1u << h;
                 }
                 const uint32_t zf = (vw[root] >> kZoneShift) & 7u;
                 if ((zf & own) != own) {
@@ -586,78 +584,77 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     }
     __syncwarp();
 
-    // -- records of live seam zones, in pixel order ----------------------------
-    uint32_t live_roots = 0u;
-    {
-        uint32_t r = roots;
-        while (r) {
-            const int h = __ffs(r) - 1;
-            r &= r - 1u;
-            const uint32_t z = (vw[run_word(y, h)] >> kZoneShift) & 7u;
-            if ((z & kTouchesSeam) && (z & kDead) != kDead) {
-                live_roots |= 1u << h;
-            }
-        }
-    }
-    uint32_t nrec = 0;
-    const uint32_t rec0 = warp_prefix(__popc(live_roots), nrec);
-    const int64_t frag_base = item * kSlots;
-    {
-        uint32_t r = live_roots;
-        uint32_t rec = rec0;
-        while (r) {
-            const int h = __ffs(r) - 1;
-            r &= r - 1u;
-            const int p = run_word(y, h);
-            if (rec < static_cast<uint32_t>(kSlots)) {
-                const uint32_t w = vw[p];
-                vw[p] = w | ((rec + 1u) << kRecShift);
-                const uint32_t z = (w >> kZoneShift) & 3u;
-                const int64_t gi = frag_base + rec;
-                a.parent[gi] = static_cast<int32_t>(gi);
-                a.bits[gi] = z | (z << kLocalShift);
-            } else {
-                err = kErrFragmentOverflow;
-            }
-            ++rec;
-        }
-    }
-    __syncwarp();
-
     // -- listed pixels: verdicts of settled zones, run log of live zones ------
     // Per row (lane y): `hmax` / `hmin` collect the heads of the runs of
     // settled zones whose maxima / minima byte is 255; `vmax` / `vmin` are
-    // those runs' pixels.
+    // those runs' pixels.  A live seam zone gets its record (fragment) when
+    // the loop first meets one of its runs: one lane per root takes the
+    // next number, in the order of the loop's steps and lanes.
     uint32_t* plog = a.pending + item * kPendingCap;
     int nlog = 0;
+    uint32_t nrec = 0;
+    const int64_t frag_base = item * kSlots;
     {
         // Runs that hold a dead pixel, or both a pixel with a greater and
         // one with a smaller neighbour, are in a decided zone: 0 in both
         // masks, nothing to log; only the other runs are visited.
         uint32_t r = loop_heads & undecided;
         while (__any_sync(~0u, r != 0u)) {
-            bool logged = false;
-            uint32_t entry = 0u;
+            bool live = false;
+            int h = 0, root = 0;
+            uint32_t rec1 = 0u;
             if (r) {
-                const int h = __ffs(r) - 1;
+                h = __ffs(r) - 1;
                 r &= r - 1u;
                 const int p = run_word(y, h);
-                const int root = rparent(vw[p], p);
+                root = rparent(vw[p], p);
                 const uint32_t w = vw[root];
                 const uint32_t z = (w >> kZoneShift) & 7u;
-                const bool live = (z & kTouchesSeam) && (z & kDead) != kDead;
+                live = (z & kTouchesSeam) && (z & kDead) != kDead;
                 if (live) {
-                    const uint32_t rec1 = (w >> kRecShift) & 0xFFu;
-                    if (rec1) {
-                        const int e = __ffs(ends & ~((1u << h) - 1u)) - 1;
-                        logged = true;
-                        entry = pending_entry(static_cast<int>(rec1 - 1u), h,
-                                              y, e - h + 1);
-                    }
+                    rec1 = (w >> kRecShift) & 0xFFu;
                 } else {
                     hmax |= (z & kHasGreater) ? 0u : 1u << h;
                     hmin |= (z & kHasSmaller) ? 0u : 1u << h;
                 }
+            }
+            const bool need = live && rec1 == 0u;
+            if (__any_sync(~0u, need)) {
+                // Lanes on the same new root: the lowest one numbers it.
+                const uint32_t same =
+                    __match_any_sync(~0u, need ? root : -1 - lane);
+                const int leader = __ffs(same) - 1;
+                const bool lead = need && leader == lane;
+                const uint32_t leads = __ballot_sync(~0u, lead);
+                uint32_t mine = 0u;
+                if (lead) {
+                    const uint32_t rec = nrec + __popc(leads & lt_mask);
+                    if (rec < static_cast<uint32_t>(kSlots)) {
+                        const uint32_t w = vw[root];
+                        vw[root] = w | ((rec + 1u) << kRecShift);
+                        const uint32_t z = (w >> kZoneShift) & 3u;
+                        const int64_t gi = frag_base + rec;
+                        a.parent[gi] = static_cast<int32_t>(gi);
+                        a.bits[gi] = z | (z << kLocalShift);
+                        mine = rec + 1u;
+                    } else {
+                        err = kErrFragmentOverflow;
+                    }
+                }
+                const uint32_t got = __shfl_sync(~0u, mine, leader);
+                if (need) {
+                    rec1 = got;
+                }
+                nrec += __popc(leads);
+                __syncwarp();
+            }
+            bool logged = false;
+            uint32_t entry = 0u;
+            if (live && rec1) {
+                const int e = __ffs(ends & ~((1u << h) - 1u)) - 1;
+                logged = true;
+                entry = pending_entry(static_cast<int>(rec1 - 1u), h, y,
+                                      e - h + 1);
             }
             const uint32_t bal = __ballot_sync(~0u, logged);
             if (logged) {
