@@ -510,20 +510,47 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             partners = 0u;
         }
         linked = m | partners;
-        while (__any_sync(~0u, m != 0u)) {
-            if (m) {
-                const int x = __ffs(m) - 1;
-                m &= m - 1u;
+        // A run's first contact (lowest column; a carry from the run's head
+        // stops at it) makes the partner above its parent with a plain
+        // store: the lane writes only its own row's still-zero words, and
+        // the parent lies in the row above, so the forest keeps every root
+        // the smallest word of its tree.
+        const uint32_t first = ((((cont >> 1) & ~m) + heads) & m);
+        {
+            uint32_t f = first;
+#pragma unroll 1
+            while (f) {
+                const int x = __ffs(f) - 1;
+                f &= f - 1u;
+                const int xp = ((A >> x) & 1u) ? x
+                             : ((B >> x) & 1u) ? x - 1 : x + 1;
                 const int p = run_word(y, head_of(heads, x));
-                if (((A | B) >> x) & 1u) {
+                vw[p] = with_parent(0u, p,
+                                    run_word(y - 1, head_of(headsm1, xp)));
+            }
+        }
+        __syncwarp();
+        // Every other contact: a union (a first contact that was A or B and
+        // also C still owes its C union).
+        uint32_t rest_ab = (A | B) & ~first;
+        uint32_t rest_c = C & ~(first & ~(A | B));
+        while (__any_sync(~0u, (rest_ab | rest_c) != 0u)) {
+            const uint32_t rest = rest_ab | rest_c;
+            if (rest) {
+                const int x = __ffs(rest) - 1;
+                const uint32_t bit = 1u << x;
+                const int p = run_word(y, head_of(heads, x));
+                if (rest_ab & bit) {
                     const int xp = ((A >> x) & 1u) ? x : x - 1;
                     runion(sm.word, p, run_word(y - 1, head_of(headsm1, xp)),
                            err);
                 }
-                if ((C >> x) & 1u) {
+                if (rest_c & bit) {
                     runion(sm.word, p,
                            run_word(y - 1, head_of(headsm1, x + 1)), err);
                 }
+                rest_ab &= ~bit;
+                rest_c &= ~bit;
             }
         }
     }
