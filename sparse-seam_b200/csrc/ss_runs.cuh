@@ -171,9 +171,10 @@ __device__ __forceinline__ void store_rows(uint8_t* omax, uint8_t* omin,
                                            int64_t out_pitch, uint32_t mxb,
                                            uint32_t mnb, int vec) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
-    const int per_row = T / vec;
-    const int c = lane % per_row;
-    const int rr = lane / per_row;
+    // vec is 16, 8 or 4: shifts instead of divides.
+    const int lv = 31 - __clz(vec);
+    const int c = lane & ((T >> lv) - 1);
+    const int rr = lane >> (5 - lv);
     for (int r0 = 0; r0 < T; r0 += vec) {
         const int r = r0 + rr;
         const uint32_t bx = __shfl_sync(~0u, mxb, r) >> (c * vec);
