@@ -369,7 +369,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         unsigned hmin_c = min(min(static_cast<unsigned>(Lc),
                                   static_cast<unsigned>(vc)),
                               static_cast<unsigned>(Rc));
-#pragma unroll 2
+#pragma unroll 4
         for (int y = 0; y < g.th; ++y) {
             const int16_t* nrow = scol + (y + 2) * kHaloW;
             const int Ln = nrow[0];
@@ -592,18 +592,23 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                                      ((own_lt >> h) & 1u) * kHasSmaller |
                                      ((own_seam >> h) & 1u) * kTouchesSeam;
                 const int p = run_word(y, h);
+                // The walk keeps the root's word: the flags read from it may
+                // lag other lanes' ORs, which only costs a redundant OR.
+                const uint32_t wp = vw[p];
+                uint32_t wr = wp;
                 int root = p;
 #pragma unroll 1
                 for (int it = 0; it < T * T; ++it) {
-                    const int up = rparent(vw[root], root);
+                    const int up = rparent(wr, root);
                     if (up == root) break;
                     root = up;
+                    wr = vw[root];
                 }
                 if (root != p) {
                     // p is not a root: no other lane writes its word now.
-                    vw[p] = with_parent(vw[p], p, root);
+                    vw[p] = with_parent(wp, p, root);
                 }
-                const uint32_t zf = (vw[root] >> kZoneShift) & 7u;
+                const uint32_t zf = (wr >> kZoneShift) & 7u;
                 if ((zf & own) != own) {
                     atomicOr(sm.word + root, own << kZoneShift);
                 }
