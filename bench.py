@@ -893,7 +893,11 @@ def uneven_section(args, pkg, device, stream):
                zip(maxs + mins, ref_max + ref_min))
     out["autotuned"] = {
         "gpix_s": round(pixels / ms / 1e6, 3), "ms": round(ms, 4),
-        "launches": len(tb.parts), "tuning_s": round(tune_s, 1),
+        "launches": 1 if tb.single is not None else len(tb.parts),
+        "form": ("one default launch (faster than the tuned choices on "
+                 "this batch)" if tb.single is not None
+                 else "the tuned choices"),
+        "tuning_s": round(tune_s, 1),
         "choices": {str(k): v.label() for k, v in table.choices.items()},
         "class_bounds_px": list(at.CLASS_BOUNDS[:-1]),
     }

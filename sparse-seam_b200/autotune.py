@@ -187,7 +187,11 @@ class TunedBatch:
     parts run concurrently, each on its own stream forked from and joined
     back into the caller's stream with events, so the GPU fills its SMs from
     all parts at once; the fork and join are captured into a CUDA graph like
-    any other stream work.
+    any other stream work.  When the batch splits into several parts, the
+    split and one launch over the whole batch are timed on it once, at
+    construction, and `run` uses the faster form (`single` is set when that
+    is the one launch).  The same check guards a one-part batch whose tuned
+    choice is not the library default.
     """
 
     def __init__(self, images: Sequence, maxima: Sequence, minima: Sequence,
@@ -215,10 +219,40 @@ class TunedBatch:
         device = images[0].device if len(images) else None
         self._streams = [torch.cuda.Stream(device)
                          for _ in self.parts[1:]]
+        # Choices tuned on one class's sample at a time need not carry over
+        # to this batch (a seam/resolve grouping fitted to the sample's
+        # launch size, or a split slower than one launch): unless the tuned
+        # form is already the library default over the whole batch, both are
+        # timed on the batch once and the faster is kept.
+        self.single = None
+        default = (len(self.parts) == 1 and
+                   self.parts[0][0].warps == _pkg.get_kernel_config(
+                       self.parts[0][0].tile) and
+                   not self.parts[0][0].persistent and
+                   self.parts[0][0].group == 0)
+        if self.parts and not default:
+            tiles = [c.tile for c in table.choices.values()]
+            tile = max(set(tiles), key=tiles.count) if tiles else 32
+            plan = _pkg.BatchPlan(list(images), list(maxima), list(minima),
+                                  tile=tile, stream=stream)
+            ws = plan.make_workspace(stream=stream)
+            main = stream or torch.cuda.current_stream()
+            t_split = _time_on(main, self._run_parts)
+            t_single = _time_on(main, lambda s: plan.run(ws, stream=s))
+            if t_single < t_split:
+                self.single = (plan, ws)
 
     def run(self, stream=None) -> None:
         import torch
         main = stream or torch.cuda.current_stream()
+        if self.single is not None:
+            plan, ws = self.single
+            plan.run(ws, stream=main)
+            return
+        self._run_parts(main)
+
+    def _run_parts(self, main) -> None:
+        import torch
         fork = torch.cuda.Event()
         fork.record(main)
         joins = []
@@ -237,5 +271,22 @@ class TunedBatch:
             main.wait_event(done)
 
     def read_status(self, stream=None) -> None:
+        if self.single is not None:
+            self.single[1].read_status(stream)
+            return
         for _, _, ws in self.parts:
             ws.read_status(stream)
+
+
+def _time_on(stream, fn, reps: int = 3) -> float:
+    """Device milliseconds of one call of fn(stream), after one warm-up."""
+    import torch
+    fn(stream)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(reps):
+        fn(stream)
+    end.record(stream)
+    end.synchronize()
+    return start.elapsed_time(end) / reps

@@ -163,12 +163,19 @@ def test_autotuned_batch_matches_oracle():
     maxs = [torch.empty_like(i) for i in images]
     mins = [torch.empty_like(i) for i in images]
     tb = at.TunedBatch(images, maxs, mins, table)
-    tb.run()
-    tb.read_status()
-    for i, im in enumerate(images):
-        want = oracle.extrema(im.cpu().numpy())
-        assert np.array_equal(maxs[i].cpu().numpy(), want[0]), i
-        assert np.array_equal(mins[i].cpu().numpy(), want[1]), i
+    wants = [oracle.extrema(im.cpu().numpy()) for im in images]
+    # The form `run` picked, then the split by size class itself.
+    for form in (tb.run,
+                 lambda: tb._run_parts(torch.cuda.current_stream())):
+        for m in maxs + mins:
+            m.fill_(5)
+        form()
+        torch.cuda.synchronize()
+        for part in tb.parts:
+            part[2].read_status()
+        for i, want in enumerate(wants):
+            assert np.array_equal(maxs[i].cpu().numpy(), want[0]), i
+            assert np.array_equal(mins[i].cpu().numpy(), want[1]), i
 
 
 @pytest.mark.parametrize("group", [1, 2, 8, 32])
