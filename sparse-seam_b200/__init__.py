@@ -202,7 +202,7 @@ SIGNATURES = {
 
 
 def read_image(path: str) -> np.ndarray:
-    """An image file (PGM, PNG, BMP or JPEG) as a 2-D uint8 array, 8-bit gray as the
+    """An image file (PGM, PNG, BMP, JPEG or TIFF) as a 2-D uint8 array, 8-bit gray as the
     reference's cv::imread(path, IMREAD_GRAYSCALE) reads it."""
     w, h = _I(0), _I(0)
     p = os.fsencode(path)

@@ -2,7 +2,7 @@
 
 Compiles ``csrc/ss_route.cu`` (the route), ``csrc/ss_server.cu`` (the
 serving loop), ``csrc/ss_pack.cu`` (compact mask transfer, host side with
-OpenMP) and ``csrc/ss_image_io.cpp`` (PGM / PNG / BMP / JPEG files, zlib) into ``libsparseseam.so`` next to this file with
+OpenMP) and ``csrc/ss_image_io.cpp`` (PGM / PNG / BMP / JPEG / TIFF files, zlib) into ``libsparseseam.so`` next to this file with
 nvcc.  The library has a plain C ABI (``include/sparse_seam.h``) and links the
 CUDA runtime statically, so it loads into any process on the GPU host, with or
 without PyTorch.

@@ -8,8 +8,8 @@
 //              [--device=0] [--block=16] [--warmup=5] [--reps=30]
 //              [--tile=32] [--masks]
 //
-// For every .pgm / .png / .bmp / .jpg / .jpeg file of <image_dir> (sorted by
-// name): the image is
+// For every .pgm / .png / .bmp / .jpg / .jpeg / .tif / .tiff file of
+// <image_dir> (sorted by name): the image is
 // read as 8-bit gray, copied to the device once, run `warmup` times, then
 // `reps` times timed with CUDA events (compute: device-resident input) and
 // `reps` times timed on the host clock from the host image to both host
@@ -90,11 +90,11 @@ std::vector<uint8_t> read_image(const fs::path& p, int& w, int& h) {
     return px;
 }
 
-// Expected mask of `stem` in `dir` (.pgm, else .png, else .bmp), or an empty
-// vector.
+// Expected mask of `stem` in `dir` (.pgm, else .png, else .bmp, else .tif), or
+// an empty vector.
 std::vector<uint8_t> expected(const fs::path& dir, const std::string& stem,
                               int w, int h) {
-    for (const char* ext : {".pgm", ".png", ".bmp"}) {
+    for (const char* ext : {".pgm", ".png", ".bmp", ".tif"}) {
         const fs::path p = dir / (stem + ext);
         if (fs::exists(p)) {
             int ew = 0, eh = 0;
@@ -209,7 +209,8 @@ int main(int argc, char** argv) {
             const std::string ext = e.path().extension().string();
             if (e.is_regular_file() &&
                 (ext == ".pgm" || ext == ".png" || ext == ".bmp" ||
-                 ext == ".jpg" || ext == ".jpeg")) {
+                 ext == ".jpg" || ext == ".jpeg" || ext == ".tif" ||
+                 ext == ".tiff")) {
                 files.push_back(e.path());
             }
         }

@@ -2,9 +2,11 @@
 // serving loop: PGM (P5 binary, P2 ASCII), PNG (every colour type, bit
 // depths 1, 2, 4 and 8, all five scanline filters, not interlaced), BMP
 // (1-, 4- and 8-bit palettes, 16-bit 5-5-5 / 5-6-5, 24- and 32-bit, RLE8 and
-// RLE4, core and V1-V5 headers) and JPEG (baseline / extended sequential
+// RLE4, core and V1-V5 headers), JPEG (baseline / extended sequential
 // Huffman, 8-bit, gray or YCbCr, any sampling, restart intervals, EXIF
-// orientation), read as one byte per pixel; PGM (P5) written.
+// orientation) and TIFF (strips or tiles; none, LZW, Deflate, PackBits;
+// predictor; 1/8/16-bit gray, 8-bit RGB(A) and palette; orientation), read as
+// one byte per pixel; PGM (P5) written.
 //
 // The reference reads images with OpenCV, cv::imread(path,
 // IMREAD_GRAYSCALE) (harness/primary/snapshot_sparse_seam_cuda_v1_0.cu:87-103,
@@ -1067,6 +1069,299 @@ ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
     return SS_OK;
 }
 
+// ---- TIFF ------------------------------------------------------------------
+// First image of the file, chunky samples in strips or tiles, compression
+// none, LZW, Deflate or PackBits, horizontal-difference predictor.  Gray as
+// OpenCV returns it (each rule checked against OpenCV 4.13): 1-bit samples
+// scale to 0 / 255; 16-bit samples keep their high byte; MinIsWhite is
+// inverted; a gray image's alpha is ignored; 8-bit RGB and palette colours
+// (16-bit map entries, high byte) take the BMP weights, and RGB with
+// unassociated alpha is premultiplied first, (c a + 127) / 255; the
+// Orientation tag is applied.  4-bit, 16-bit colour, planar, floating-point
+// and JPEG-compressed images are refused.
+
+uint32_t tiff_u16(const uint8_t* p, bool le) {
+    return le ? le16(p) : (uint32_t(p[0]) << 8) | p[1];
+}
+
+uint32_t tiff_u32(const uint8_t* p, bool le) {
+    return le ? le32(p)
+              : (uint32_t(p[0]) << 24) | (uint32_t(p[1]) << 16) |
+                    (uint32_t(p[2]) << 8) | p[3];
+}
+
+// TIFF LZW: MSB-first codes of 9..12 bits, 256 = clear, 257 = end, the code
+// width growing one code early.
+bool tiff_lzw(const uint8_t* in, size_t n, std::vector<uint8_t>& out,
+              size_t want) {
+    std::vector<uint16_t> prefix(4096);
+    std::vector<uint8_t> suffix(4096), first(4096);
+    std::vector<uint8_t> stack(4096);
+    for (int i = 0; i < 256; ++i) {
+        suffix[i] = first[i] = static_cast<uint8_t>(i);
+    }
+    int next = 258, width = 9, old = -1;
+    uint32_t acc = 0;
+    int have = 0;
+    size_t pos = 0;
+    out.clear();
+    while (out.size() < want) {
+        while (have < width) {
+            if (pos >= n) {
+                return out.size() >= want;
+            }
+            acc = (acc << 8) | in[pos++];
+            have += 8;
+        }
+        const int code = static_cast<int>((acc >> (have - width)) &
+                                          ((1u << width) - 1u));
+        have -= width;
+        if (code == 257) {
+            break;
+        }
+        if (code == 256) {
+            next = 258;
+            width = 9;
+            old = -1;
+            continue;
+        }
+        int c = code, sp = 0;
+        uint8_t firstc;
+        if (old < 0) {
+            if (code > 255) {
+                return false;
+            }
+            out.push_back(static_cast<uint8_t>(code));
+            old = code;
+            continue;
+        }
+        if (code < next) {
+            firstc = first[code];
+        } else if (code == next) {
+            firstc = first[old];
+            stack[sp++] = firstc;
+            c = old;
+        } else {
+            return false;
+        }
+        while (c > 255) {
+            stack[sp++] = suffix[c];
+            c = prefix[c];
+        }
+        stack[sp++] = static_cast<uint8_t>(c);
+        while (sp) {
+            out.push_back(stack[--sp]);
+        }
+        if (next < 4096) {
+            prefix[next] = static_cast<uint16_t>(old);
+            suffix[next] = firstc;
+            first[next] = first[old];
+            ++next;
+        }
+        if (next + 1 >= (1 << width) && width < 12) {
+            ++width;
+        }
+        old = code;
+    }
+    return out.size() >= want;
+}
+
+bool tiff_packbits(const uint8_t* in, size_t n, std::vector<uint8_t>& out,
+                   size_t want) {
+    out.clear();
+    size_t pos = 0;
+    while (pos < n && out.size() < want) {
+        const int c = static_cast<int8_t>(in[pos++]);
+        if (c >= 0) {
+            if (pos + c + 1 > n) return false;
+            out.insert(out.end(), in + pos, in + pos + c + 1);
+            pos += c + 1;
+        } else if (c != -128) {
+            if (pos >= n) return false;
+            out.insert(out.end(), static_cast<size_t>(1 - c), in[pos++]);
+        }
+    }
+    return out.size() >= want;
+}
+
+ss_status decode_tiff(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
+                      int& w, int& h) {
+    const size_t n = d.size();
+    if (n < 8) return SS_ERR_INVALID_VALUE;
+    const bool le = d[0] == 'I';
+    if (tiff_u16(&d[2], le) != 42) return SS_ERR_INVALID_VALUE;
+    const size_t ifd = tiff_u32(&d[4], le);
+    if (ifd + 2 > n) return SS_ERR_INVALID_VALUE;
+    const uint32_t count = tiff_u16(&d[ifd], le);
+    if (ifd + 2 + size_t(count) * 12 > n) return SS_ERR_INVALID_VALUE;
+    // Values of an entry (BYTE, SHORT or LONG).
+    auto values = [&](size_t e, std::vector<uint32_t>& v) -> bool {
+        const uint32_t type = tiff_u16(&d[e + 2], le);
+        const uint32_t cnt = tiff_u32(&d[e + 4], le);
+        const size_t size = type == 1 ? 1 : type == 3 ? 2 : type == 4 ? 4 : 0;
+        if (!size || cnt > (1u << 24)) return false;
+        size_t at = e + 8;
+        if (size * cnt > 4) {
+            at = tiff_u32(&d[e + 8], le);
+            if (at + size * cnt > n) return false;
+        }
+        v.resize(cnt);
+        for (uint32_t i = 0; i < cnt; ++i) {
+            const uint8_t* q = &d[at + i * size];
+            v[i] = size == 1 ? q[0] : size == 2 ? tiff_u16(q, le)
+                                                : tiff_u32(q, le);
+        }
+        return true;
+    };
+    int64_t width = 0, height = 0;
+    uint32_t bps = 1, comp = 1, phot = 1, spp = 1, planar = 1, pred = 1;
+    uint32_t rps = 0xFFFFFFFFu, tile_w = 0, tile_h = 0, orientation = 1;
+    uint32_t extra = 0xFFFFFFFFu, sample_format = 1;
+    std::vector<uint32_t> offsets, counts, colormap, v;
+    for (uint32_t k = 0; k < count; ++k) {
+        const size_t e = ifd + 2 + size_t(k) * 12;
+        const uint32_t tag = tiff_u16(&d[e], le);
+        if (!values(e, v) || v.empty()) {
+            continue;   // unknown types belong to tags not used here
+        }
+        switch (tag) {
+            case 256: width = v[0]; break;
+            case 257: height = v[0]; break;
+            case 258: bps = v[0]; break;
+            case 259: comp = v[0]; break;
+            case 262: phot = v[0]; break;
+            case 274: orientation = v[0]; break;
+            case 277: spp = v[0]; break;
+            case 278: rps = v[0]; break;
+            case 284: planar = v[0]; break;
+            case 317: pred = v[0]; break;
+            case 320: colormap = v; break;
+            case 322: tile_w = v[0]; break;
+            case 323: tile_h = v[0]; break;
+            case 338: extra = v[0]; break;
+            case 339: sample_format = v[0]; break;
+            case 273: case 324: offsets = v; break;
+            case 279: case 325: counts = v; break;
+            default: break;
+        }
+    }
+    const bool gray = phot <= 1 && (spp == 1 || spp == 2);
+    const bool rgb = phot == 2 && (spp == 3 || spp == 4) && bps == 8;
+    const bool pal = phot == 3 && spp == 1 && bps == 8 &&
+                     colormap.size() == 3 * 256;
+    if (width <= 0 || height <= 0 || width * height > (int64_t(1) << 31) ||
+        planar != 1 || sample_format != 1 || (pred != 1 && pred != 2) ||
+        !(gray || rgb || pal) ||
+        !(bps == 8 || (bps == 16 && gray) || (bps == 1 && spp == 1)) ||
+        (comp != 1 && comp != 5 && comp != 8 && comp != 32946 &&
+         comp != 32773) ||
+        offsets.empty() || offsets.size() != counts.size()) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    const size_t W = size_t(width), H = size_t(height);
+    const bool tiled = tile_w > 0 && tile_h > 0;
+    const size_t bw = tiled ? tile_w : W;                 // block width
+    const size_t bh = tiled ? tile_h : std::min<size_t>(rps, H);
+    const size_t across = tiled ? (W + bw - 1) / bw : 1;
+    const size_t down = (H + bh - 1) / bh;
+    if (offsets.size() < across * down) return SS_ERR_INVALID_VALUE;
+    const size_t row_bytes = (bw * spp * bps + 7) / 8;
+    // All samples of the image, one row after another (row_out bytes).
+    const size_t row_out = (W * spp * bps + 7) / 8;
+    std::vector<uint8_t> img(row_out * H), buf;
+    for (size_t by = 0; by < down; ++by) {
+        for (size_t bx = 0; bx < across; ++bx) {
+            const size_t k = by * across + bx;
+            const size_t rows = tiled ? bh : std::min(bh, H - by * bh);
+            const size_t want = row_bytes * rows;
+            const size_t at = offsets[k], len = counts[k];
+            if (at > n || len > n - at) return SS_ERR_INVALID_VALUE;
+            const uint8_t* src = d.data() + at;
+            bool ok = true;
+            if (comp == 1) {
+                ok = len >= want;
+                buf.assign(src, src + std::min(len, want));
+            } else if (comp == 5) {
+                ok = tiff_lzw(src, len, buf, want);
+            } else if (comp == 32773) {
+                ok = tiff_packbits(src, len, buf, want);
+            } else {
+                buf.resize(want);
+                uLongf out_len = static_cast<uLongf>(want);
+                ok = uncompress(buf.data(), &out_len, src,
+                                static_cast<uLong>(len)) == Z_OK &&
+                     out_len == want;
+            }
+            if (!ok || buf.size() < want) return SS_ERR_INVALID_VALUE;
+            for (size_t r = 0; r < rows; ++r) {
+                uint8_t* row = buf.data() + r * row_bytes;
+                if (pred == 2) {   // undo horizontal differencing
+                    if (bps == 8) {
+                        for (size_t i = spp; i < bw * spp; ++i) {
+                            row[i] = static_cast<uint8_t>(row[i] + row[i - spp]);
+                        }
+                    } else if (bps == 16) {
+                        for (size_t i = spp; i < bw * spp; ++i) {
+                            const uint32_t a = tiff_u16(row + 2 * i, le) +
+                                               tiff_u16(row + 2 * (i - spp), le);
+                            row[2 * i + (le ? 0 : 1)] = static_cast<uint8_t>(a);
+                            row[2 * i + (le ? 1 : 0)] =
+                                static_cast<uint8_t>(a >> 8);
+                        }
+                    } else {
+                        return SS_ERR_INVALID_VALUE;
+                    }
+                }
+                const size_t y = by * bh + r;
+                if (y >= H) break;
+                // Columns of this block inside the image, in bytes.
+                const size_t x0 = bx * bw;
+                const size_t cols = std::min(bw, W - x0);
+                const size_t o0 = (x0 * spp * bps) / 8;
+                const size_t ob = (cols * spp * bps + 7) / 8;
+                std::memcpy(img.data() + y * row_out + o0, row, ob);
+            }
+        }
+    }
+    px.resize(W * H);
+    for (size_t y = 0; y < H; ++y) {
+        const uint8_t* s = img.data() + y * row_out;
+        uint8_t* o = px.data() + y * W;
+        for (size_t x = 0; x < W; ++x) {
+            uint32_t g;
+            if (bps == 1) {
+                g = ((s[x / 8] >> (7 - x % 8)) & 1u) ? 255u : 0u;
+            } else if (gray) {
+                g = bps == 16 ? tiff_u16(s + 2 * x * spp, le) >> 8
+                              : s[x * spp];
+            } else if (pal) {
+                const uint32_t i = s[x];
+                g = bgr_gray(colormap[512 + i] >> 8, colormap[256 + i] >> 8,
+                             colormap[i] >> 8);
+            } else {
+                uint32_t r = s[x * spp], gg = s[x * spp + 1],
+                         b = s[x * spp + 2];
+                if (spp == 4 && extra == 2) {   // unassociated alpha
+                    const uint32_t a = s[x * spp + 3];
+                    r = (r * a + 127) / 255;
+                    gg = (gg * a + 127) / 255;
+                    b = (b * a + 127) / 255;
+                }
+                g = bgr_gray(static_cast<int>(b), static_cast<int>(gg),
+                             static_cast<int>(r));
+            }
+            if (phot == 0) {
+                g = 255u - g;   // MinIsWhite
+            }
+            o[x] = static_cast<uint8_t>(g);
+        }
+    }
+    w = static_cast<int>(width);
+    h = static_cast<int>(height);
+    orient(px, w, h, static_cast<int>(orientation));
+    return SS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1089,6 +1384,12 @@ ss_status ss_read_image(const char* path, uint8_t* pixels, size_t capacity,
         st = decode_bmp(data, px, w, h);
     } else if (data.size() >= 2 && data[0] == 0xFF && data[1] == 0xD8) {
         st = decode_jpeg(data, px, w, h);
+    } else if (data.size() >= 4 &&
+               ((data[0] == 'I' && data[1] == 'I' && data[2] == 42 &&
+                 data[3] == 0) ||
+                (data[0] == 'M' && data[1] == 'M' && data[2] == 0 &&
+                 data[3] == 42))) {
+        st = decode_tiff(data, px, w, h);
     } else {
         st = decode_pgm(data, px, w, h);
     }

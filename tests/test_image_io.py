@@ -402,3 +402,234 @@ def test_jpeg_refusals(tmp_path):
         p.write_bytes(data)
         with pytest.raises(pkg.SparseSeamError):
             pkg.read_image(str(p))
+
+
+# ---- TIFF -------------------------------------------------------------------
+
+def _packbits(raw: bytes) -> bytes:
+    out = bytearray()
+    i = 0
+    while i < len(raw):
+        j = i
+        while j + 1 < len(raw) and raw[j + 1] == raw[i] and j - i < 127:
+            j += 1
+        if j > i:
+            out += bytes([(257 - (j - i + 1)) & 0xFF, raw[i]])
+            i = j + 1
+        else:
+            k = i
+            while (k + 1 < len(raw) and k - i < 127 and
+                   not (k + 2 < len(raw) and raw[k + 1] == raw[k + 2])):
+                k += 1
+            out += bytes([k - i]) + raw[i:k + 1]
+            i = k + 1
+    return bytes(out)
+
+
+def write_tiff(path, rows, width, height, spp, bps, photometric,
+               compression=1, colormap=None, predictor=1, rows_per_strip=None,
+               tile=None, little=True, extra=()):
+    """A one-image TIFF: `rows` are the packed sample bytes of each image row
+    (top first; after differencing when predictor is 2).  `tile` = (tw, th)
+    writes tiles (padded with zeros) instead of strips."""
+    e = "<" if little else ">"
+    row_bytes = (width * spp * bps + 7) // 8
+
+    def pack(block: bytes) -> bytes:
+        if compression == 8:
+            return zlib.compress(block)
+        if compression == 32773:
+            return b"".join(_packbits(block[k:k + bw_bytes])
+                            for k in range(0, len(block), bw_bytes))
+        return block
+
+    blocks = []
+    if tile:
+        tw, th = tile
+        bw_bytes = (tw * spp * bps + 7) // 8
+        for ty in range(0, height, th):
+            for tx in range(0, width, tw):
+                block = bytearray()
+                for y in range(ty, ty + th):
+                    r = rows[y] if y < height else bytes(row_bytes)
+                    part = r[tx * spp * bps // 8:(tx + tw) * spp * bps // 8]
+                    block += part + bytes(bw_bytes - len(part))
+                blocks.append(pack(bytes(block)))
+    else:
+        bw_bytes = row_bytes
+        rps = rows_per_strip or height
+        for y0 in range(0, height, rps):
+            blocks.append(pack(b"".join(rows[y0:y0 + rps])))
+    entries = [(256, 4, [width]), (257, 4, [height]), (258, 3, [bps] * spp),
+               (259, 3, [compression]), (262, 3, [photometric]),
+               (277, 3, [spp]), (284, 3, [1])]
+    if tile:
+        entries += [(322, 3, [tile[0]]), (323, 3, [tile[1]])]
+    else:
+        entries.append((278, 4, [rows_per_strip or height]))
+    if predictor != 1:
+        entries.append((317, 3, [predictor]))
+    if colormap is not None:
+        entries.append((320, 3, [int(v) for v in colormap]))
+    entries += list(extra)
+    out = bytearray((b"II" if little else b"MM") + struct.pack(e + "HI", 42, 0))
+    offsets = []
+    for b in blocks:
+        offsets.append(len(out))
+        out += b + (b"\0" if len(b) % 2 else b"")
+    entries += [(324 if tile else 273, 4, offsets),
+                (325 if tile else 279, 4, [len(b) for b in blocks])]
+    entries.sort()
+    far = {}
+    for tag, typ, vals in entries:
+        fmt = "H" if typ == 3 else "I"
+        if struct.calcsize(fmt) * len(vals) > 4:
+            far[tag] = len(out)
+            out += struct.pack(e + fmt * len(vals), *vals)
+    ifd = len(out)
+    out += struct.pack(e + "H", len(entries))
+    for tag, typ, vals in entries:
+        fmt = "H" if typ == 3 else "I"
+        if tag in far:
+            out += struct.pack(e + "HHII", tag, typ, len(vals), far[tag])
+        else:
+            v = struct.pack(e + fmt * len(vals), *vals)
+            out += struct.pack(e + "HHI", tag, typ, len(vals)) + v
+            out += bytes(4 - len(v))
+    out += struct.pack(e + "I", 0)
+    out[4:8] = struct.pack(e + "I", ifd)
+    with open(path, "wb") as f:
+        f.write(bytes(out))
+
+
+def _tiff_cases(rng):
+    """(name, writer kwargs, rows) for a spread of layouts and kinds."""
+    h, w = 37, 29
+    g8 = rng.integers(0, 256, size=(h, w)).astype(np.uint8)
+    rows8 = [g8[y].tobytes() for y in range(h)]
+    diff = np.concatenate([g8[:, :1], np.diff(g8.astype(np.int16), axis=1)],
+                          axis=1).astype(np.uint8)
+    rowsd = [diff[y].tobytes() for y in range(h)]
+    g16 = rng.integers(0, 65536, size=(h, w)).astype(np.uint16)
+    rgb = rng.integers(0, 256, size=(h, w, 3)).astype(np.uint8)
+    rgba = rng.integers(0, 256, size=(h, w, 4)).astype(np.uint8)
+    ga = rng.integers(0, 256, size=(h, w, 2)).astype(np.uint8)
+    bits = rng.integers(0, 2, size=(h, w))
+    rows1 = []
+    for y in range(h):
+        s = "".join(str(int(b)) for b in bits[y]) + "0" * (-w % 8)
+        rows1.append(bytes(int(s[i:i + 8], 2) for i in range(0, len(s), 8)))
+    cmap = rng.integers(0, 65536, size=3 * 256)
+    base = dict(width=w, height=h)
+    yield "gray8", dict(base, spp=1, bps=8, photometric=1), rows8
+    yield "gray8_strips_packbits", dict(base, spp=1, bps=8, photometric=1,
+                                        compression=32773,
+                                        rows_per_strip=5), rows8
+    yield "gray8_deflate_pred", dict(base, spp=1, bps=8, photometric=1,
+                                     compression=8, predictor=2,
+                                     rows_per_strip=7), rowsd
+    yield "gray8_tiles", dict(base, spp=1, bps=8, photometric=1,
+                              tile=(16, 16)), rows8
+    yield "gray8_tiles_deflate", dict(base, spp=1, bps=8, photometric=1,
+                                      tile=(16, 32), compression=8), rows8
+    yield "gray8_big_endian", dict(base, spp=1, bps=8, photometric=1,
+                                   little=False), rows8
+    yield "miniswhite8", dict(base, spp=1, bps=8, photometric=0), rows8
+    for little in (True, False):
+        yield f"gray16_{little}", dict(base, spp=1, bps=16, photometric=1,
+                                       little=little), [
+            g16[y].astype("<u2" if little else ">u2").tobytes()
+            for y in range(h)]
+    yield "miniswhite16", dict(base, spp=1, bps=16, photometric=0), [
+        g16[y].astype("<u2").tobytes() for y in range(h)]
+    yield "bilevel", dict(base, spp=1, bps=1, photometric=1), rows1
+    yield "bilevel_white", dict(base, spp=1, bps=1, photometric=0), rows1
+    yield "gray_alpha", dict(base, spp=2, bps=8, photometric=1,
+                             extra=[(338, 3, [2])]), [
+        ga[y].tobytes() for y in range(h)]
+    yield "rgb", dict(base, spp=3, bps=8, photometric=2), [
+        rgb[y].tobytes() for y in range(h)]
+    yield "rgb_tiles_packbits", dict(base, spp=3, bps=8, photometric=2,
+                                     tile=(16, 16), compression=32773), [
+        rgb[y].tobytes() for y in range(h)]
+    for es in (0, 1, 2):
+        yield f"rgba_es{es}", dict(base, spp=4, bps=8, photometric=2,
+                                   extra=[(338, 3, [es])]), [
+            rgba[y].tobytes() for y in range(h)]
+    yield "palette", dict(base, spp=1, bps=8, photometric=3,
+                          colormap=cmap), rows8
+    for o in range(1, 5):
+        yield f"orientation{o}", dict(base, spp=1, bps=8, photometric=1,
+                                      extra=[(274, 3, [o])]), rows8
+    # Orientations that swap the axes: OpenCV 4.13 reads them from square
+    # images only (it fails on other shapes).
+    square = [g8[y, :w].tobytes() for y in range(w)]
+    for o in range(5, 9):
+        yield f"orientation{o}", dict(width=w, height=w, spp=1, bps=8,
+                                      photometric=1,
+                                      extra=[(274, 3, [o])]), square
+
+
+def test_tiff_matches_opencv(tmp_path):
+    cv2 = pytest.importorskip("cv2")
+    pkg = package()
+    rng = np.random.default_rng(21)
+    for name, kw, rows in _tiff_cases(rng):
+        path = str(tmp_path / f"{name}.tif")
+        write_tiff(path, rows, **kw)
+        want = cv2.imread(path, cv2.IMREAD_GRAYSCALE)
+        assert want is not None, name
+        got = pkg.read_image(path)
+        assert got.shape == want.shape, name
+        assert np.array_equal(got, want), (name, int((got != want).sum()))
+
+
+@pytest.mark.parametrize("compression", [1, 5, 8, 32773])
+@pytest.mark.parametrize("predictor", [1, 2])
+def test_tiff_written_by_opencv(tmp_path, compression, predictor):
+    """LZW and the other codecs as OpenCV's own TIFF writer makes them."""
+    cv2 = pytest.importorskip("cv2")
+    pkg = package()
+    rng = np.random.default_rng(compression + predictor)
+    yy, xx = np.mgrid[0:61, 0:47]
+    smooth = ((xx * 3 + yy * 5) % 256).astype(np.uint8)
+    for k, img in enumerate((smooth,
+                             rng.integers(0, 256, size=(61, 47, 3)).astype(
+                                 np.uint8),
+                             (smooth.astype(np.uint16) * 257))):
+        path = str(tmp_path / f"cv{k}.tif")
+        params = [cv2.IMWRITE_TIFF_COMPRESSION, compression,
+                  cv2.IMWRITE_TIFF_ROWSPERSTRIP, 8]
+        if predictor == 2 and compression in (5, 8):
+            params += [cv2.IMWRITE_TIFF_PREDICTOR, 2]
+        assert cv2.imwrite(path, img, params)
+        want = cv2.imread(path, cv2.IMREAD_GRAYSCALE)
+        got = pkg.read_image(path)
+        assert got.shape == want.shape, k
+        assert np.array_equal(got, want), (k, int((got != want).sum()))
+
+
+def test_tiff_refusals(tmp_path):
+    pkg = package()
+    rng = np.random.default_rng(3)
+    rgb16 = rng.integers(0, 65536, size=(8, 8, 3)).astype("<u2")
+    cases = {
+        "rgb16": (dict(width=8, height=8, spp=3, bps=16, photometric=2),
+                  [rgb16[y].tobytes() for y in range(8)]),
+        "gray4": (dict(width=8, height=8, spp=1, bps=4, photometric=1),
+                  [bytes(4)] * 8),
+        "jpeg": (dict(width=8, height=8, spp=1, bps=8, photometric=1,
+                      compression=7), [bytes(8)] * 8),
+    }
+    for name, (kw, rows) in cases.items():
+        path = str(tmp_path / f"{name}.tif")
+        write_tiff(path, rows, **kw)
+        with pytest.raises(pkg.SparseSeamError):
+            pkg.read_image(path)
+    cut = tmp_path / "cut.tif"
+    write_tiff(str(cut), [bytes(range(8))] * 8, width=8, height=8, spp=1,
+               bps=8, photometric=1)
+    data = cut.read_bytes()
+    cut.write_bytes(data[:20])
+    with pytest.raises(pkg.SparseSeamError):
+        pkg.read_image(str(cut))
