@@ -369,7 +369,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         unsigned hmin_c = min(min(static_cast<unsigned>(Lc),
                                   static_cast<unsigned>(vc)),
                               static_cast<unsigned>(Rc));
-#pragma unroll 4
+#pragma unroll 8
         for (int y = 0; y < g.th; ++y) {
             const int16_t* nrow = scol + (y + 2) * kHaloW;
             const int Ln = nrow[0];
