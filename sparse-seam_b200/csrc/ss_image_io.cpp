@@ -25,6 +25,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -658,7 +659,7 @@ uint8_t idct_limit(int64_t x) {
 
 // 8 x 8 inverse DCT of dequantised coefficients (natural order) into
 // `out` (row stride `stride`).
-void idct_islow(const int32_t* in, uint8_t* out, size_t stride) {
+void idct_islow(const int64_t* in, uint8_t* out, size_t stride) {
     // sqrt(2) times cosine combinations (c_k = cos(k pi / 16)), x 2^13:
     constexpr int64_t k0_298 = 2446;    // -c1 + c3 + c5 - c7
     constexpr int64_t k0_390 = 3196;    // c3 - c5
@@ -682,8 +683,9 @@ void idct_islow(const int32_t* in, uint8_t* out, size_t stride) {
         int64_t z1 = (z2 + z3) * k0_541;
         const int64_t t2 = z1 - z3 * k1_847;
         const int64_t t3 = z1 + z2 * k0_765;
-        const int64_t t0 = (x[0] + x[4]) << kConst;
-        const int64_t t1 = (x[0] - x[4]) << kConst;
+        // Multiplications, not shifts: the sums may be negative.
+        const int64_t t0 = (x[0] + x[4]) * (int64_t(1) << kConst);
+        const int64_t t1 = (x[0] - x[4]) * (int64_t(1) << kConst);
         const int64_t t10 = t0 + t3, t13 = t0 - t3;
         const int64_t t11 = t1 + t2, t12 = t1 - t2;
         int64_t o0 = x[7], o1 = x[5], o2 = x[3], o3 = x[1];
@@ -969,7 +971,7 @@ ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
                 }
             }
             JpegBits br{d.data(), n, pos};
-            int pred[4] = {0, 0, 0, 0};
+            int64_t pred[4] = {0, 0, 0, 0};   // 64-bit: hostile files
             // Units: interleaved MCUs, or the blocks of the one component.
             int units_x, units_y;
             if (ns > 1) {
@@ -981,7 +983,7 @@ ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
                 units_x = (cw + 7) / 8;
                 units_y = (ch + 7) / 8;
             }
-            int32_t coef[64];
+            int64_t coef[64];
             int64_t unit = 0;
             for (int uy = 0; uy < units_y; ++uy) {
                 for (int ux = 0; ux < units_x; ++ux, ++unit) {
@@ -1021,7 +1023,7 @@ ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
                                         return SS_ERR_INVALID_VALUE;
                                     }
                                     const int nat = kZigzag[z];
-                                    coef[nat] = extend(br.bits(sz), sz) * q[nat];
+                                    coef[nat] = int64_t(extend(br.bits(sz), sz)) * q[nat];
                                     ++z;
                                 }
                                 if (k != 0) {
@@ -1366,11 +1368,12 @@ ss_status decode_tiff(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
 
 extern "C" {
 
-ss_status ss_read_image(const char* path, uint8_t* pixels, size_t capacity,
-                        int* width, int* height) {
-    if (!path || !width || !height) {
-        return SS_ERR_INVALID_VALUE;
-    }
+}  // extern "C"
+
+namespace {
+
+ss_status read_image_impl(const char* path, uint8_t* pixels, size_t capacity,
+                          int* width, int* height) {
     std::vector<uint8_t> data;
     if (!read_file(path, data)) {
         return SS_ERR_INVALID_VALUE;
@@ -1406,6 +1409,26 @@ ss_status ss_read_image(const char* path, uint8_t* pixels, size_t capacity,
     }
     std::memcpy(pixels, px.data(), px.size());
     return SS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ss_status ss_read_image(const char* path, uint8_t* pixels, size_t capacity,
+                        int* width, int* height) {
+    if (!path || !width || !height) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    // No exception crosses the C ABI: a file whose header claims more
+    // pixels than the host can hold ends here.
+    try {
+        return read_image_impl(path, pixels, capacity, width, height);
+    } catch (const std::bad_alloc&) {
+        return SS_ERR_HOST_ALLOC;
+    } catch (...) {
+        return SS_ERR_INVALID_VALUE;
+    }
 }
 
 ss_status ss_write_pgm(const char* path, const uint8_t* pixels, int width,
