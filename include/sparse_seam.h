@@ -296,7 +296,7 @@ ss_status ss_enqueue_unpack_masks(const uint32_t* h_max_bits,
 /* ---------------------------------------------------------------------- */
 /* Reads a PGM (P5 / P2, maxval <= 255), PNG (any colour type, 1/2/4/8-bit
  * samples, not interlaced), BMP (1/4/8-bit palettes, 16/24/32-bit, RLE8 /
- * RLE4), JPEG (sequential Huffman, 8-bit, gray or YCbCr; EXIF orientation
+ * RLE4), JPEG (sequential or progressive Huffman, 8-bit, gray or YCbCr; EXIF orientation
  * applied) or TIFF (strips / tiles, none / LZW / Deflate / PackBits, 1/8/16-
  * bit gray, 8-bit RGB(A) and palette) as 8-bit gray, as the reference's
  * cv::imread(path, IMREAD_GRAYSCALE) does

@@ -2,9 +2,9 @@
 // serving loop: PGM (P5 binary, P2 ASCII), PNG (every colour type, bit
 // depths 1, 2, 4 and 8, all five scanline filters, not interlaced), BMP
 // (1-, 4- and 8-bit palettes, 16-bit 5-5-5 / 5-6-5, 24- and 32-bit, RLE8 and
-// RLE4, core and V1-V5 headers), JPEG (baseline / extended sequential
-// Huffman, 8-bit, gray or YCbCr, any sampling, restart intervals, EXIF
-// orientation) and TIFF (strips or tiles; none, LZW, Deflate, PackBits;
+// RLE4, core and V1-V5 headers), JPEG (baseline / extended sequential /
+// progressive Huffman, 8-bit, gray or YCbCr, any sampling, restart
+// intervals, EXIF orientation) and TIFF (strips or tiles; none, LZW, Deflate, PackBits;
 // predictor; 1/8/16-bit gray, 8-bit RGB(A) and palette; orientation), read as
 // one byte per pixel; PGM (P5) written.
 //
@@ -500,7 +500,8 @@ ss_status decode_bmp(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
 }
 
 // ---- JPEG ------------------------------------------------------------------
-// Baseline and extended sequential Huffman JPEG, 8-bit samples.  OpenCV asks
+// Baseline, extended sequential and progressive Huffman JPEG, 8-bit
+// samples.  OpenCV asks
 // its JPEG library for gray output, which for a YCbCr (or one-component)
 // file is the luma plane itself: the Y blocks are entropy-decoded,
 // dequantised and inverse-transformed, the chroma blocks only decoded to
@@ -509,8 +510,8 @@ ss_status decode_bmp(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
 // constants x 2^13, two extra fraction bits between the column and the row
 // pass, rounding shifts, and the output offset by 128 and limited through a
 // 10-bit wrap-around table.  The EXIF orientation tag is applied as imread
-// applies it.  Progressive, lossless, arithmetic-coded and 12-bit files,
-// and colour spaces other than YCbCr / gray, are refused.
+// applies it.  Lossless, arithmetic-coded and 12-bit files, and colour
+// spaces other than YCbCr / gray, are refused.
 
 struct JpegHuff {
     int maxcode[18];
@@ -736,6 +737,136 @@ void idct_islow(const int64_t* in, uint8_t* out, size_t stride) {
     }
 }
 
+// One block of a scan into c (natural order, coefficients before
+// dequantisation).  Sequential files: the whole block.  Progressive files
+// (ITU-T T.81 G.1.2): a DC first scan sets the DC term to the running
+// prediction << Al, a DC refinement ORs in bit Al; an AC first scan sets band
+// Ss..Se (value << Al) with end-of-band runs spanning blocks; an AC
+// refinement adds bit Al to the band's nonzero terms (one correction bit
+// each, in zig-zag order) and places new +-2^Al terms after the given
+// number of zero terms.
+bool decode_block(JpegBits& br, int32_t* c, bool progressive, int ss, int se,
+                  int ah, int al, const JpegHuff& dct, const JpegHuff& act,
+                  int64_t& pred, int64_t& eobrun) {
+    if (!progressive || ss == 0) {
+        if (progressive && ah > 0) {
+            if (br.bits(1)) {
+                c[0] |= 1 << al;
+            }
+        } else {
+            const int t = dct.defined ? br.decode(dct) : -1;
+            if (t < 0 || t > 11) {
+                return false;
+            }
+            pred += t ? extend(br.bits(t), t) : 0;
+            c[0] = static_cast<int32_t>(pred * (int64_t(1) << al));
+        }
+        if (progressive) {
+            return true;
+        }
+        for (int z = 1; z < 64;) {
+            const int rs = br.decode(act);
+            if (rs < 0) {
+                return false;
+            }
+            const int r = rs >> 4, sz = rs & 15;
+            if (sz == 0) {
+                if (r != 15) break;   // end of block
+                z += 16;
+                continue;
+            }
+            z += r;
+            if (z > 63) {
+                return false;
+            }
+            c[kZigzag[z]] = extend(br.bits(sz), sz);
+            ++z;
+        }
+        return true;
+    }
+    if (ah == 0) {   // AC first scan
+        if (eobrun > 0) {
+            --eobrun;
+            return true;
+        }
+        for (int k = ss; k <= se; ++k) {
+            const int rs = br.decode(act);
+            if (rs < 0) {
+                return false;
+            }
+            const int r = rs >> 4, sz = rs & 15;
+            if (sz) {
+                k += r;
+                if (k > se) {
+                    return false;
+                }
+                c[kZigzag[k]] =
+                    static_cast<int32_t>(extend(br.bits(sz), sz) * (1 << al));
+            } else if (r < 15) {
+                eobrun = (int64_t(1) << r) - 1 + (r ? br.bits(r) : 0);
+                break;
+            } else {
+                k += 15;
+            }
+        }
+        return true;
+    }
+    // AC refinement.
+    const int32_t p1 = 1 << al, m1 = -p1;
+    auto refine = [&](int32_t& v) {
+        if (br.bits(1) && (v & p1) == 0) {
+            v += v >= 0 ? p1 : m1;
+        }
+    };
+    int k = ss;
+    if (eobrun == 0) {
+        for (; k <= se; ++k) {
+            const int rs = br.decode(act);
+            if (rs < 0) {
+                return false;
+            }
+            int r = rs >> 4;
+            const int sz = rs & 15;
+            int32_t value = 0;
+            if (sz) {
+                if (sz != 1) {
+                    return false;
+                }
+                value = br.bits(1) ? p1 : m1;
+            } else if (r != 15) {
+                eobrun = (int64_t(1) << r) + (r ? br.bits(r) : 0);
+                break;
+            }
+            // Skip r zero terms (refining the nonzero ones met on the way),
+            // then place the new term, if any.
+            for (; k <= se; ++k) {
+                int32_t& v = c[kZigzag[k]];
+                if (v != 0) {
+                    refine(v);
+                } else if (r-- == 0) {
+                    break;
+                }
+            }
+            if (value) {
+                if (k > se) {
+                    return false;
+                }
+                c[kZigzag[k]] = value;
+            }
+        }
+    }
+    if (eobrun > 0) {
+        for (; k <= se; ++k) {
+            int32_t& v = c[kZigzag[k]];
+            if (v != 0) {
+                refine(v);
+            }
+        }
+        --eobrun;
+    }
+    return true;
+}
+
 // EXIF orientation (tag 0x0112 of IFD0) from an APP1 payload, 1 if none.
 int exif_orientation(const uint8_t* p, size_t len) {
     if (len < 14 || std::memcmp(p, "Exif\0\0", 6) != 0) {
@@ -815,7 +946,11 @@ ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
     } comps[4];
     int ncomp = 0, width = 0, height = 0, restart = 0, orientation = 1;
     bool adobe_rgb = false;
-    std::vector<uint8_t> plane;
+    // The luma blocks' coefficients in natural order, before dequantisation
+    // (a progressive file fills them over several scans).
+    std::vector<int32_t> ycoef;
+    bool progressive = false;
+    int64_t eobrun = 0;
     size_t plane_w = 0;
     int y_blocks_w = 0, y_blocks_h = 0, hmax = 1, vmax = 1;
     bool y_done = false;
@@ -887,7 +1022,8 @@ ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
                 return SS_ERR_INVALID_VALUE;
             }
             restart = (seg[0] << 8) | seg[1];
-        } else if (m == 0xC0 || m == 0xC1) {
+        } else if (m == 0xC0 || m == 0xC1 || m == 0xC2) {
+            progressive = m == 0xC2;
             if (sl < 6 || seg[0] != 8) {
                 return SS_ERR_INVALID_VALUE;
             }
@@ -922,12 +1058,12 @@ ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
             y_blocks_w = mcus_x * hmax;
             y_blocks_h = mcus_y * vmax;
             plane_w = size_t(y_blocks_w) * 8;
-            plane.assign(plane_w * size_t(y_blocks_h) * 8, 0);
-        } else if ((m >= 0xC2 && m <= 0xCF) && m != 0xC4 && m != 0xC8 &&
+            ycoef.assign(size_t(y_blocks_w) * size_t(y_blocks_h) * 64, 0);
+        } else if ((m >= 0xC3 && m <= 0xCF) && m != 0xC4 && m != 0xC8 &&
                    m != 0xCC) {
-            return SS_ERR_INVALID_VALUE;   // progressive, lossless, arithmetic
+            return SS_ERR_INVALID_VALUE;   // lossless, arithmetic
         } else if (m == 0xDA) {
-            if (plane.empty() || sl < 1) {
+            if (ycoef.empty() || sl < 1) {
                 return SS_ERR_INVALID_VALUE;
             }
             const int ns = seg[0];
@@ -949,9 +1085,14 @@ ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
                 }
                 has_y = has_y || sc[i] == 0;
             }
-            const uint8_t ss = seg[1 + 2 * ns], se = seg[2 + 2 * ns],
-                          a = seg[3 + 2 * ns];
-            if (ss != 0 || se != 63 || a != 0) {
+            const int ss = seg[1 + 2 * ns], se = seg[2 + 2 * ns];
+            const int ah = seg[3 + 2 * ns] >> 4, al = seg[3 + 2 * ns] & 15;
+            if (!progressive) {
+                if (ss != 0 || se != 63 || ah != 0 || al != 0) {
+                    return SS_ERR_INVALID_VALUE;
+                }
+            } else if (se > 63 || ss > se || (ss == 0 && se != 0) ||
+                       (ss > 0 && ns != 1) || al > 13 || ah > 13) {
                 return SS_ERR_INVALID_VALUE;
             }
             pos += len;
@@ -963,15 +1104,20 @@ ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
                 }
                 continue;
             }
+            const bool dc_scan = !progressive || ss == 0;
+            const bool ac_scan = !progressive || ss > 0;
             for (int i = 0; i < ns; ++i) {
-                const int k = sc[i];
-                if (!dc[std_dc[i]].defined || !ac[std_ac[i]].defined ||
-                    !qt_defined[comps[k].tq]) {
+                if ((dc_scan && ah == 0 && !dc[std_dc[i]].defined) ||
+                    (ac_scan && !ac[std_ac[i]].defined)) {
                     return SS_ERR_INVALID_VALUE;
                 }
             }
+            if (!qt_defined[comps[0].tq]) {
+                return SS_ERR_INVALID_VALUE;
+            }
             JpegBits br{d.data(), n, pos};
             int64_t pred[4] = {0, 0, 0, 0};   // 64-bit: hostile files
+            eobrun = 0;
             // Units: interleaved MCUs, or the blocks of the one component.
             int units_x, units_y;
             if (ns > 1) {
@@ -983,7 +1129,7 @@ ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
                 units_x = (cw + 7) / 8;
                 units_y = (ch + 7) / 8;
             }
-            int64_t coef[64];
+            int32_t scratch[64];
             int64_t unit = 0;
             for (int uy = 0; uy < units_y; ++uy) {
                 for (int ux = 0; ux < units_x; ++ux, ++unit) {
@@ -992,6 +1138,7 @@ ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
                             return SS_ERR_INVALID_VALUE;
                         }
                         pred[0] = pred[1] = pred[2] = pred[3] = 0;
+                        eobrun = 0;
                     }
                     for (int i = 0; i < ns; ++i) {
                         const int k = sc[i];
@@ -999,44 +1146,24 @@ ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
                         const int bv = ns > 1 ? comps[k].vs : 1;
                         for (int by = 0; by < bv; ++by) {
                             for (int bx = 0; bx < bh; ++bx) {
-                                std::memset(coef, 0, sizeof(coef));
-                                const int t = br.decode(dc[std_dc[i]]);
-                                if (t < 0 || t > 11) {
-                                    return SS_ERR_INVALID_VALUE;
-                                }
-                                pred[i] += t ? extend(br.bits(t), t) : 0;
-                                const uint16_t* q = qt[comps[k].tq];
-                                coef[0] = pred[i] * q[0];
-                                for (int z = 1; z < 64;) {
-                                    const int rs = br.decode(ac[std_ac[i]]);
-                                    if (rs < 0) {
-                                        return SS_ERR_INVALID_VALUE;
-                                    }
-                                    const int r = rs >> 4, sz = rs & 15;
-                                    if (sz == 0) {
-                                        if (r != 15) break;   // end of block
-                                        z += 16;
-                                        continue;
-                                    }
-                                    z += r;
-                                    if (z > 63) {
-                                        return SS_ERR_INVALID_VALUE;
-                                    }
-                                    const int nat = kZigzag[z];
-                                    coef[nat] = int64_t(extend(br.bits(sz), sz)) * q[nat];
-                                    ++z;
-                                }
-                                if (k != 0) {
-                                    continue;
-                                }
+                                // The block's coefficients: a luma block of
+                                // the image, else scratch (decoded to keep
+                                // the bit stream in step, then dropped).
                                 const int gx = ns > 1 ? ux * hmax + bx : ux;
                                 const int gy = ns > 1 ? uy * vmax + by : uy;
-                                if (gx < y_blocks_w && gy < y_blocks_h) {
-                                    idct_islow(coef,
-                                               plane.data() + size_t(gy) * 8 *
-                                                                  plane_w +
-                                                   size_t(gx) * 8,
-                                               plane_w);
+                                int32_t* c = scratch;
+                                if (k == 0 && gx < y_blocks_w && gy < y_blocks_h) {
+                                    c = ycoef.data() +
+                                        (size_t(gy) * y_blocks_w + gx) * 64;
+                                }
+                                if (c == scratch) {
+                                    std::memset(scratch, 0, sizeof(scratch));
+                                }
+                                if (!decode_block(br, c, progressive, ss, se,
+                                                  ah, al, dc[std_dc[i]],
+                                                  ac[std_ac[i]], pred[i],
+                                                  eobrun)) {
+                                    return SS_ERR_INVALID_VALUE;
                                 }
                             }
                         }
@@ -1059,6 +1186,20 @@ ss_status decode_jpeg(const std::vector<uint8_t>& d, std::vector<uint8_t>& px,
     }
     if (!y_done || (ncomp == 3 && adobe_rgb)) {
         return SS_ERR_INVALID_VALUE;
+    }
+    // Dequantise and inverse-transform every luma block.
+    std::vector<uint8_t> plane(plane_w * size_t(y_blocks_h) * 8);
+    const uint16_t* q = qt[comps[0].tq];
+    int64_t block[64];
+    for (int gy = 0; gy < y_blocks_h; ++gy) {
+        for (int gx = 0; gx < y_blocks_w; ++gx) {
+            const int32_t* c = ycoef.data() + (size_t(gy) * y_blocks_w + gx) * 64;
+            for (int z = 0; z < 64; ++z) {
+                block[z] = int64_t(c[z]) * q[z];
+            }
+            idct_islow(block, plane.data() + size_t(gy) * 8 * plane_w + size_t(gx) * 8,
+                       plane_w);
+        }
     }
     px.resize(size_t(width) * height);
     for (int y = 0; y < height; ++y) {

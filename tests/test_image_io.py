@@ -328,6 +328,7 @@ JPEG_PARAMS = [
     ("411", "IMWRITE_JPEG_SAMPLING_FACTOR", "IMWRITE_JPEG_SAMPLING_FACTOR_411"),
     ("restart3", "IMWRITE_JPEG_RST_INTERVAL", 3),
     ("optimised", "IMWRITE_JPEG_OPTIMIZE", 1),
+    ("progressive", "IMWRITE_JPEG_PROGRESSIVE", 1),
 ]
 
 
@@ -387,15 +388,41 @@ def test_jpeg_exif_orientation(tmp_path):
             assert np.array_equal(got, want), (o, little)
 
 
+def test_jpeg_progressive_variants(tmp_path):
+    """Progressive files with restart intervals, chroma subsampling and
+    qualities from 10 to 100 (spectral selection and successive
+    approximation scans, end-of-band runs)."""
+    cv2 = pytest.importorskip("cv2")
+    pkg = package()
+    rng = np.random.default_rng(14)
+    k = 0
+    for img in _jpeg_inputs(rng):
+        for q in (10, 60, 100):
+            for extra in ([], [cv2.IMWRITE_JPEG_RST_INTERVAL, 2],
+                          [cv2.IMWRITE_JPEG_SAMPLING_FACTOR,
+                           cv2.IMWRITE_JPEG_SAMPLING_FACTOR_420]):
+                ok, buf = cv2.imencode(".jpg", img,
+                                       [cv2.IMWRITE_JPEG_PROGRESSIVE, 1,
+                                        cv2.IMWRITE_JPEG_QUALITY, q] + extra)
+                path = str(tmp_path / f"p{k}.jpg")
+                k += 1
+                with open(path, "wb") as f:
+                    f.write(buf.tobytes())
+                want = cv2.imread(path, cv2.IMREAD_GRAYSCALE)
+                got = pkg.read_image(path)
+                assert got.shape == want.shape, (k, q, extra)
+                assert np.array_equal(got, want), (k, q, extra,
+                                                   int((got != want).sum()))
+
+
 def test_jpeg_refusals(tmp_path):
     cv2 = pytest.importorskip("cv2")
     pkg = package()
     rng = np.random.default_rng(13)
     img = rng.integers(0, 256, size=(40, 40, 3)).astype(np.uint8)
-    ok, prog = cv2.imencode(".jpg", img, [cv2.IMWRITE_JPEG_PROGRESSIVE, 1])
     ok, base = cv2.imencode(".jpg", img)
-    files = {"progressive": prog.tobytes(),
-             "truncated": base.tobytes()[:len(base) // 2],
+    # (A progressive file cut between scans is a valid, less refined image.)
+    files = {"truncated": base.tobytes()[:len(base) // 2],
              "no_frame": b"\xff\xd8\xff\xd9"}
     for name, data in files.items():
         p = tmp_path / f"{name}.jpg"
