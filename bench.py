@@ -579,6 +579,9 @@ def main():
     seam_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
     resolve_ms = statistics.mean(e[2].elapsed_time(e[3]) for e in ev)
     ws.read_status(stream)
+    # Seam statistics of one step (the flip counter accumulates until read).
+    plan.run(ws, persistent=persistent, stream=stream)
+    step_stats = ws.read_status(stream)
     hbm, peak_kind = peaks()
     achieved = BYTES_PER_PIXEL * pixels / (tile_ms / 1e3) / 1e9
     traffic = committed_traffic()
@@ -609,9 +612,12 @@ def main():
         "route_roofline_frac": round(
             BYTES_PER_PIXEL * pixels / (ms_total / args.steps / 1e3) / 1e9
             / hbm, 4),
-        "stats": {"active_fragments": int(stats.active_fragments),
-                  "tiles": int(stats.tiles),
-                  "flipped_tiles_per_step": None},
+        "stats": {"active_fragments": int(step_stats.active_fragments),
+                  "tiles": int(step_stats.tiles),
+                  "flipped_tiles_per_step": int(step_stats.flipped_tiles),
+                  "live_pixels_per_step": int(step_stats.live_pixels),
+                  "seam_pixel_fraction": round(
+                      step_stats.live_pixels / max(1, pixels), 5)},
         "clocks": clock_info,
         "checked_images": len(idx),
         "mismatches": mismatches,

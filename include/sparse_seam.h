@@ -116,6 +116,11 @@ typedef struct ss_stats {
     uint64_t tiles;               /* tiles of the last call */
     uint64_t flipped_tiles;       /* tiles whose seam fragments changed
                                      verdict after the global merge */
+    uint64_t live_pixels;         /* pixels whose verdict waited for the
+                                     global merge (the runs of live seam
+                                     zones; row-scan kernels only, else 0):
+                                     the seam-pixel share is this over the
+                                     call's pixels */
 } ss_stats;
 
 /* Kernel configuration used for a tile size by every later call of this

@@ -66,6 +66,7 @@ class Stats(ctypes.Structure):
         ("active_fragments", ctypes.c_uint64),
         ("tiles", ctypes.c_uint64),
         ("flipped_tiles", ctypes.c_uint64),
+        ("live_pixels", ctypes.c_uint64),
     ]
 
 

@@ -65,7 +65,9 @@ struct Header {
     uint32_t flipped_tiles;  // tiles rewritten by the resolve pass
     uint32_t tile;           // tile edge of the last call
     uint64_t last_tiles;     // tiles of the last call
-    uint64_t reserved[27];
+    uint32_t route;          // 1: the last call ran the row-scan kernels
+    uint32_t pad;
+    uint64_t reserved[26];
 };
 static_assert(sizeof(Header) == 256, "header is one 256-byte block");
 
@@ -132,7 +134,8 @@ struct Arena {
     int32_t* parent;         // [g * 4T + record]: fragment union-find
     uint32_t* bits;          // [g * 4T + record]: bits 0-1 zone flags (the
                              //   component's at a root), bits 8-9 own flags
-    uint32_t* pending_count; // [g]: run-log entries (row-scan path)
+    uint32_t* pending_count; // [g]: run-log entries in bits 0-15, their
+                             //   pixels in bits 16-31 (row-scan path)
     uint32_t* pending;       // [g * T * T + e]: run-log entries
     uint32_t* seam_count;    // [g]: seam items (row-scan path)
     uint32_t* seam_items;    // [g * 12T + i]: seam items (row-scan path)

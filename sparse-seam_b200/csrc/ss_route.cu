@@ -263,6 +263,7 @@ tile_pass_kernel(Source src, Arena a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.header->last_tiles = static_cast<uint64_t>(src.total_tiles);
         a.header->tile = T;
+        a.header->route = 0u;
     }
     if constexpr (kPersistent) {
         for (;;) {
@@ -451,6 +452,7 @@ runs_tile_pass_kernel(Source src, Arena a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.header->last_tiles = static_cast<uint64_t>(src.total_tiles);
         a.header->tile = rowscan::T;
+        a.header->route = 1u;
     }
     if constexpr (kPersistent) {
         for (;;) {
@@ -1013,6 +1015,23 @@ ss_status ss_read_status(void* d_workspace, size_t workspace_bytes,
                 sum += c;
             }
             stats->active_fragments = sum;
+            if (h.route == 1u && h.tile == 32u) {
+                // Pixels of the logged runs: bits 16-31 of each tile's
+                // run-log count.
+                std::vector<uint32_t> logs(h.last_tiles);
+                if (cudaMemcpy(logs.data(),
+                               static_cast<char*>(d_workspace) +
+                                   L.pending_count,
+                               logs.size() * sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost) != cudaSuccess) {
+                    return SS_ERR_CUDA;
+                }
+                uint64_t px = 0;
+                for (uint32_t c : logs) {
+                    px += c >> 16;
+                }
+                stats->live_pixels = px;
+            }
         }
     }
     // Clear the error word, its detail and the flip counter.

@@ -349,7 +349,8 @@ __device__ __forceinline__ void resolve_group(ResolveSmem& sm,
     const int64_t tile = first + lane;
     const bool valid = lane < src.group && tile < src.total_tiles;
     const uint32_t n =
-        valid ? min(a.pending_count[tile], static_cast<uint32_t>(kPendingCap))
+        valid ? min(a.pending_count[tile] & 0xFFFFu,
+                    static_cast<uint32_t>(kPendingCap))
               : 0u;
     const uint32_t k = n ? min(static_cast<uint32_t>(a.fragment_count[tile]),
                                static_cast<uint32_t>(kSlots))

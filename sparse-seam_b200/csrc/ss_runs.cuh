@@ -625,6 +625,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     // next number, in the order of the loop's steps and lanes.
     uint32_t* plog = a.pending + item * kPendingCap;
     int nlog = 0;
+    uint32_t live_px = 0u;   // pixels of this lane's logged runs
     uint32_t nrec = 0;
     const int64_t frag_base = item * kSlots;
     {
@@ -688,6 +689,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                 logged = true;
                 entry = pending_entry(static_cast<int>(rec1 - 1u), h, y,
                                       e - h + 1);
+                live_px += static_cast<uint32_t>(e - h + 1);
             }
             const uint32_t bal = __ballot_sync(~0u, logged);
             if (logged) {
@@ -698,6 +700,8 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     }
     const uint32_t vmax = run_span(shape, hmax);
     const uint32_t vmin = run_span(shape, hmin);
+    // The tile's logged pixels (a statistic: bits 16-31 of its log count).
+    const uint32_t logged_px = __reduce_add_sync(~0u, live_px);
     // The mask bytes of every pixel of the tile.  Pixels of live zones get a
     // placeholder 0 here and their final bytes from the resolve pass, which
     // runs after this pass; so whole rows are written, with 16-, 8- or
@@ -833,7 +837,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     if (lane == 0) {
         a.fragment_count[item] =
             static_cast<uint16_t>(min(nrec, static_cast<uint32_t>(kSlots)));
-        a.pending_count[item] = static_cast<uint32_t>(nlog);
+        a.pending_count[item] = static_cast<uint32_t>(nlog) | (logged_px << 16);
         a.seam_count[item] = static_cast<uint32_t>(nitems);
     }
     if (err) {

@@ -281,3 +281,36 @@ def test_every_store_width(kernel_config):
             # Bytes between the rows are left alone.
             pad = base_mx[shift:shift + h * pitch].view(h, pitch)[:, w:]
             assert (pad == 9).all(), f"{name} pitch {pitch}: wrote padding"
+
+
+def test_seam_statistics():
+    """The status's statistics: a constant image is one zone that crosses
+    every seam (every pixel waits for the merge), a one-tile image has no
+    seam, and a batch's counts are its images' sums."""
+    pkg = package()
+    flat = torch.full((300, 200), 77, dtype=torch.uint8, device="cuda")
+    small = torch.randint(0, 256, (32, 32), dtype=torch.uint8, device="cuda")
+    noisy = torch.randint(0, 4, (256, 320), dtype=torch.uint8, device="cuda")
+    per = []
+    for im in (flat, small, noisy):
+        mx, mn = torch.empty_like(im), torch.empty_like(im)
+        plan = pkg.BatchPlan([im], [mx], [mn], tile=32)
+        ws = plan.make_workspace()
+        plan.run(ws)
+        st = ws.read_status()
+        per.append(st)
+        assert st.tiles == ((im.shape[0] + 31) // 32) * ((im.shape[1] + 31) // 32)
+    assert per[0].live_pixels == flat.numel()
+    assert per[0].active_fragments == per[0].tiles
+    assert per[1].live_pixels == 0 and per[1].active_fragments == 0
+    assert 0 < per[2].live_pixels <= noisy.numel()
+    images = [flat, small, noisy]
+    maxs = [torch.empty_like(i) for i in images]
+    mins = [torch.empty_like(i) for i in images]
+    plan = pkg.BatchPlan(images, maxs, mins, tile=32)
+    ws = plan.make_workspace()
+    plan.run(ws)
+    st = ws.read_status()
+    assert st.live_pixels == sum(p.live_pixels for p in per)
+    assert st.active_fragments == sum(p.active_fragments for p in per)
+    assert st.tiles == sum(p.tiles for p in per)
