@@ -76,6 +76,8 @@ def parse_args():
                    help="re-quantise the corpus to this many gray levels")
     p.add_argument("--sweep", action="store_true",
                    help="add the quantisation x tile sweep of the corpus")
+    p.add_argument("--serve-seconds", type=float, default=60.0,
+                   help="duration of each Poisson rate of the served stream")
     return p.parse_args()
 
 
@@ -469,6 +471,9 @@ def main():
         return rc
     from importlib import import_module
     pkg = import_module("sparse-seam_b200")
+    serving = not args.quick and not args.no_extra and dist.world == 1
+    # Worker processes are spawned before the first GPU call.
+    plateau_pool, plateau = start_plateau_maps() if serving else (None, None)
     device = torch.device("cuda", dist.local)
     torch.cuda.set_device(device)
     tile = args.tile
@@ -632,18 +637,64 @@ def main():
             # Single-GPU workloads (the uneven-size batch, the served stream
             # and the resolution sweep are defined on one B200).
             line["batched_uneven"] = uneven_section(args, pkg, device, stream)
-            line["served"] = serving_section(args, pkg, device, stream)
+            line["served"] = serving_section(args, pkg, device, stream,
+                                             plateau)
+            plateau_pool.shutdown()
             line["resolution_sweep"] = resolution_section(args, pkg, device,
                                                           stream, hbm)
     elif dist.rank == 0:
         line["cpu_baseline"] = None
         line["e2e"] = None
 
+    line["results"] = summary(line)
     del graph
     if dist.rank == 0:
         print(json.dumps(line))
     dist.close()
     return 0
+
+
+def summary(line):
+    """The compact results, placed last in the JSON line (readers that keep
+    only its end still see them): Gpix/s unless stated."""
+    def get(*path):
+        d = line
+        for k in path:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+    out = {
+        "batched": line.get("value"),
+        "per_image": get("per_image", "value"),
+        "single_2040x1356_us": get("single_image_2040x1356", "us_per_image"),
+        "single_2040x1356": get("single_image_2040x1356", "gpix_s"),
+        "launch_floor_us_1_4": [get("launch_floor_2040x1356", "us_1_launch"),
+                                get("launch_floor_2040x1356", "us_4_launch")],
+        "e2e": get("e2e", "value"),
+        "tile_pass_frac": get("roofline", "frac"),
+    }
+    for t in (32, 64):
+        out[f"ref_protocol_t{t}"] = {
+            "product": get("ref_protocol", f"t{t}", "product", "gpix_s"),
+            "sparse_seam": get("ref_protocol", f"t{t}", "reference",
+                               "sparse_seam_v1_0", "value"),
+            "global_uf": get("ref_protocol", f"t{t}", "reference",
+                             "global_uf", "value")}
+    out["uneven"] = {k: get("batched_uneven", k, "gpix_s")
+                     for k in ("per_image", "batched_grid",
+                               "batched_persistent", "autotuned")}
+    rates = get("served", "rates_req_s") or {}
+    out["served"] = {r: [v.get("p50_ms"), v.get("p99_ms"), v.get("gpix_s")]
+                     for r, v in rates.items()}
+    out["served_note"] = "rate: [p50 ms, p99 ms, Gpix/s]"
+    out["served_duration_s"] = get("served", "duration_s")
+    out["served_vs_per_image_h2h"] = [get("served", "saturated", "gpix_s"),
+                                      get("served", "per_image_h2h",
+                                          "gpix_s")]
+    out["cpu_baseline"] = get("cpu_baseline", "value")
+    out["mismatches"] = line.get("mismatches")
+    return out
 
 
 def sweep(args, pkg, images, stream):
@@ -803,7 +854,102 @@ def secondary(args, pkg, plan, images, host_images, maxs, mins, stream, dist,
         }
         sample = [host_images[i] for i in (0, 1, 2, 3, 4)] + \
             [host_images[i] for i in range(len(images) - 5, len(images))]
-        out["reference_gpu"] = reference_gpu_routes(sample, tile)
+        out["ref_protocol"] = ref_protocol_section(sample)
+        out["reference_gpu"] = out["ref_protocol"]["t32"]["reference"]
+    if large:
+        out["launch_floor_2040x1356"] = launch_floor_section(
+            pkg, images[0].device, stream, len(large), args.warmup,
+            args.steps)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Launch floor and the reference's per-image protocol
+# ---------------------------------------------------------------------------
+
+def _later_group(tiles: int, sms: int) -> int:
+    """Tiles per CTA of the later passes, as the library chooses them."""
+    group = 1
+    while group < 32 and tiles > group * sms * 8:
+        group *= 2
+    return group
+
+
+def launch_floor_section(pkg, device, stream, n_images, warmup, reps):
+    """Graph replay of 1 and of 4 empty kernels per 2040x1356 image, with the
+    grid shapes of the route's tile pass (2 warps per CTA, one tile per warp)
+    and later passes (8 warps per CTA): the floor no launch-based per-image
+    route goes below."""
+    import torch
+    lib = pkg.lib()
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    tiles = ((2040 + 31) // 32) * ((1356 + 31) // 32)
+    g1 = (tiles + 1) // 2
+    g2 = (tiles + _later_group(tiles, sms) - 1) // _later_group(tiles, sms)
+
+    def run(k):
+        s = ctypes.c_void_p(stream.cuda_stream)
+        for _ in range(n_images):
+            assert lib.ss_empty_launches(1, g1, 64, s) == 0
+            if k > 1:
+                assert lib.ss_empty_launches(k - 1, g2, 256, s) == 0
+
+    out = {"grids": [g1, g2]}
+    for k in (1, 4):
+        ms = _graph_ms(lambda: run(k), stream, warmup, reps)
+        out[f"us_{k}_launch"] = round(ms / n_images * 1e3, 3)
+    return out
+
+
+def _write_pgm(path, image):
+    h, w = image.shape
+    with open(path, "wb") as f:
+        f.write(b"P5\n%d %d\n255\n" % (w, h))
+        f.write(np.ascontiguousarray(image).tobytes())
+
+
+def ref_protocol_section(sample, tiles=(32, 64), warmup=5, reps=30):
+    """The product and the reference's own GPU routes on the same images with
+    the reference's protocol (README.md:169-176 of the reference): per image
+    `warmup` warm-ups and `reps` CUDA-event timed calls, no graph, median per
+    image; aggregate = sum(px) / sum(median).  The product runs through the
+    drop-in command-line harness (ss_harness, C ABI); the reference through
+    its own harness routines built for sm_100a."""
+    import csv
+    import shutil
+    import tempfile
+    harness = os.path.join(ROOT, "sparse-seam_b200", "ss_harness")
+    out = {"sample": f"{len(sample)} corpus images", "warmup": warmup,
+           "reps": reps}
+    tmp = tempfile.mkdtemp(prefix="ss_refproto_")
+    try:
+        src = os.path.join(tmp, "images")
+        os.makedirs(src)
+        for i, im in enumerate(sample):
+            _write_pgm(os.path.join(src, f"img_{i:03d}.pgm"), im)
+        for tile in tiles:
+            dst = os.path.join(tmp, f"out_t{tile}")
+            rc = subprocess.run(
+                [harness, src, f"--output={dst}", f"--warmup={warmup}",
+                 f"--reps={reps}", f"--tile={tile}"],
+                capture_output=True, text=True, timeout=900).returncode
+            entry = {}
+            if rc != 0:
+                entry["product"] = {"error": f"ss_harness exit {rc}"}
+            else:
+                with open(os.path.join(dst, "ss_harness.csv"),
+                          newline="") as f:
+                    rows = list(csv.DictReader(f))
+                px = sum(int(r["width"]) * int(r["height"]) for r in rows)
+                med = sum(float(r["median_compute_ms"]) for r in rows)
+                h2h = sum(float(r["median_h2h_ms"]) for r in rows)
+                entry["product"] = {"gpix_s": round(px / med / 1e6, 3),
+                                    "h2h_gpix_s": round(px / h2h / 1e6, 3)}
+            entry["reference"] = reference_gpu_routes(sample, tile, warmup,
+                                                      reps)
+            out[f"t{tile}"] = entry
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
     return out
 
 
@@ -922,27 +1068,48 @@ def uneven_section(args, pkg, device, stream):
 SERVE_SIZES = ((321, 481), (1024, 1024), (1356, 2040), (4096, 4096),
                (8192, 8192))
 SERVE_WEIGHTS = (0.3, 0.3, 0.2, 0.15, 0.05)
+SERVE_RATES = (50.0, 100.0, 500.0, 2000.0)   # requests per second
+SERVE_COUNTS = (8, 8, 8, 4, 4)   # distinct images per request size
 
 
-def _serve_images(device):
-    """Distinct host images per request size; generators from the
-    single-image, corpus and uneven-batch workloads (uniform 16 levels,
-    smooth noise, uniform-quantised, plateau maps; plateau maps only up to
-    2040x1356)."""
+def serve_plateau_jobs():
+    """(size index, image index, seed) of the served stream's plateau maps."""
+    return [(k, j, 1000 * k + j) for k in range(len(SERVE_SIZES))
+            for j in range(SERVE_COUNTS[k]) if j % 4 == 3]
+
+
+def start_plateau_maps():
+    """Starts the served stream's plateau maps (distance maps of 8192^2
+    ellipse masks take tens of seconds on the host) in spawned worker
+    processes, so they are ready when the serving section starts."""
+    import concurrent.futures
+    import multiprocessing
+    from importlib import import_module
+    synth = import_module("sparse-seam_b200.synth")
+    ex = concurrent.futures.ProcessPoolExecutor(
+        max_workers=4, mp_context=multiprocessing.get_context("spawn"))
+    futures = {(k, j): ex.submit(synth.plateau_map, *SERVE_SIZES[k], seed)
+               for k, j, seed in serve_plateau_jobs()}
+    return ex, futures
+
+
+def _serve_images(device, plateau):
+    """Distinct pinned host images per request size, the generators of the
+    single-image, corpus and uneven-batch workloads in turn: uniform 16
+    levels, smooth noise, uniform-quantised (2..256 levels), plateau maps."""
     import torch
     from importlib import import_module
     synth = import_module("sparse-seam_b200.synth")
-    count = {0: 8, 1: 8, 2: 8, 3: 4, 4: 2}
     pool = {}
     for k, (h, w) in enumerate(SERVE_SIZES):
         imgs = []
-        for j in range(count[k]):
+        for j in range(SERVE_COUNTS[k]):
             kind = j % 4
             seed = 1000 * k + j
             if kind == 0:
-                t = synth.smooth_noise(h, w, seed, device=device).cpu()
-            elif kind == 1:
                 t = torch.from_numpy(synth.uniform_q16(h, w, seed))
+            elif kind == 1:
+                t = synth.smooth_noise(h, w, seed, device=device).cpu()
             elif kind == 2:
                 rng = np.random.default_rng(seed)
                 levels = int(rng.integers(2, 257))
@@ -950,9 +1117,7 @@ def _serve_images(device):
                     rng.integers(0, 256, size=(h, w)).astype(np.uint8),
                     levels))
             else:
-                t = (torch.from_numpy(synth.plateau_map(h, w, seed))
-                     if h * w <= 1356 * 2040 else
-                     synth.smooth_noise(h, w, seed, device=device).cpu())
+                t = torch.from_numpy(plateau[(k, j)].result())
             p = torch.empty((h, w), dtype=torch.uint8, pin_memory=True)
             p.copy_(t)
             imgs.append(p)
@@ -960,7 +1125,7 @@ def _serve_images(device):
     return pool
 
 
-def serving_section(args, pkg, device, stream):
+def serving_section(args, pkg, device, stream, plateau):
     """Served request stream: Poisson arrivals, each request one host image
     whose size is drawn from 481x321 / 1024^2 / 2040x1356 / 4096^2 / 8192^2
     (weights 0.3 / 0.3 / 0.2 / 0.15 / 0.05).  Latency = completion (masks in
@@ -972,7 +1137,7 @@ def serving_section(args, pkg, device, stream):
     import torch
     from importlib import import_module
     serve = import_module("sparse-seam_b200.serve")
-    pool = _serve_images(device)
+    pool = _serve_images(device, plateau)
     ring = {0: 16, 1: 16, 2: 12, 3: 8, 4: 4}
     outs = {k: [(torch.empty(SERVE_SIZES[k], dtype=torch.uint8,
                              pin_memory=True),
@@ -998,17 +1163,22 @@ def serving_section(args, pkg, device, stream):
 
     cfg = dict(tile=32, persistent=True, inflight=3, max_batch_images=256,
                batch_tiles=1 << 17, pool_bytes=8 << 30)
-    out = {"workload": ("Poisson arrivals; request sizes 481x321 / 1024^2 / "
-                        "2040x1356 / 4096^2 / 8192^2 with weights "
-                        "0.3/0.3/0.2/0.15/0.05; pinned host images in, "
-                        "masks out to pinned host buffers"),
+    out = {"workload": ("Poisson arrivals at 50 / 100 / 500 / 2000 req/s; "
+                        "request sizes 481x321 / 1024^2 / 2040x1356 / "
+                        "4096^2 / 8192^2 with weights 0.3/0.3/0.2/0.15/0.05; "
+                        "generators in turn uniform 16 levels, smooth noise, "
+                        "uniform-quantised 2..256 levels, plateau maps; "
+                        "pinned host images in, masks out to pinned host "
+                        "buffers"),
+           "duration_s": float(args.serve_seconds),
            "server": {k: v for k, v in cfg.items()}}
     rates = {}
     with serve.Server(**cfg) as srv:
         warm = draw(24)
         serve.run_trace(srv, np.zeros(len(warm), dtype=np.int64),
                         maker(warm))
-        for rate, dur in ((100.0, 2.0), (500.0, 2.0), (2000.0, 2.0)):
+        dur = float(args.serve_seconds)
+        for rate in SERVE_RATES:
             arrivals = serve.poisson_trace(rate, dur, seed=int(rate))
             reqs = draw(len(arrivals))
             res = serve.run_trace(srv, arrivals, maker(reqs))

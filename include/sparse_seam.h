@@ -135,23 +135,34 @@ typedef struct ss_stats {
 ss_status ss_set_kernel_config(int tile, int warps);
 ss_status ss_get_kernel_config(int tile, int* warps);
 
+/* Measurement aid: enqueues `count` launches of an empty kernel with `grid`
+ * CTAs of `threads` threads on `stream`.  Replayed from a CUDA graph with the
+ * grid shapes of a route call, it gives the launch floor that no launch-based
+ * route can go below.  No counterpart in the reference. */
+ss_status ss_empty_launches(int count, int grid, int threads, void* stream);
+
 /* Zero-allocation form of ss_extrema, for callers that cannot allocate
  * device memory (code that must not enter the allocator: another
  * allocator's callback, a latency-critical loop, a plug-in whose host owns
  * every device allocation).  No counterpart in the reference, which always
  * allocates per image.  The route's scratch is a fixed 32 MiB array inside
- * the library, held on every GPU that loads it until the process exits; this
- * call allocates nothing (no cudaMalloc, no allocating library routine).
+ * the library; this call allocates nothing (no cudaMalloc, no allocating
+ * library routine).
  * Limits: images whose ss_workspace_bytes exceeds 32 MiB are rejected with
  * SS_ERR_EXCEEDS_STATIC_SCRATCH (at T = 32 about 4.6 Mpixel, e.g. 2040 x 1356;
- * at T = 64 about 50 Mpixel).  The first call on a device sets the array up
- * (looks up its device address with the device current, clears it, waits for
- * the clear on `stream`); make that first call before any stream capture.
+ * at T = 64 about 50 Mpixel).
+ * Set-up: the array lives in its own module, which the driver loads (and so
+ * allocates the 32 MiB) the first time this call or
+ * ss_static_scratch_read_status runs in a CUDA context; the first call in a
+ * context also clears the array and waits for the clear on `stream`.  So make
+ * a first call (a warm-up) outside the no-allocation context and before any
+ * stream capture.  The array is then held on that GPU until the process
+ * exits.
  * Every call shares the one array and it keeps the previous call's contents,
- * so each call clears what must start at zero; calls that overlap on the GPU
- * (other streams, other host threads) race and must be serialised by the
- * caller.  Device-side invariant failures are recorded in the array's header
- * and are not reported by this entry point. */
+ * so each call clears what must start at zero (including the error word);
+ * calls that overlap on the GPU (other streams, other host threads) race and
+ * must be serialised by the caller.  Device-side invariant failures of a call
+ * are read with ss_static_scratch_read_status before the next call. */
 ss_status ss_extrema_static_scratch(const uint8_t* d_image, int width,
                                     int height, int pitch, int tile,
                                     uint8_t* d_maxima, uint8_t* d_minima,
@@ -162,6 +173,13 @@ ss_status ss_extrema_static_scratch(const uint8_t* d_image, int width,
  * Returns SS_OK or the first device-side failure. */
 ss_status ss_read_status(void* d_workspace, size_t workspace_bytes,
                          void* stream, ss_stats* stats);
+
+/* ss_read_status for the array of ss_extrema_static_scratch in the current
+ * context: synchronises `stream` and returns SS_OK or the device-side
+ * failure of the last call (SS_ERR_WORKSPACE_UNINITIALIZED if no call has
+ * set the array up in this context).  Allocates no device memory.  No
+ * counterpart in the reference. */
+ss_status ss_static_scratch_read_status(void* stream, ss_stats* stats);
 
 /* Host-to-host convenience form: copies a host image to the device, runs
  * ss_extrema, copies both masks back and synchronises.  Device buffers are

@@ -177,8 +177,10 @@ SIGNATURES = {
     "ss_extrema_batch_pass": (_I, [_VP, _VP, _SZ, _I, _I, _VP, _SZ, _VP]),
     "ss_set_kernel_config": (_I, [_I, _I]),
     "ss_get_kernel_config": (_I, [_I, ctypes.POINTER(_I)]),
+    "ss_empty_launches": (_I, [_I, _I, _I, _VP]),
     "ss_extrema_static_scratch": (_I, [_VP, _I, _I, _I, _I, _VP, _VP, _I,
                                        _VP]),
+    "ss_static_scratch_read_status": (_I, [_VP, ctypes.POINTER(Stats)]),
     "ss_extrema_batch_launch": (_I, [_VP, _VP, _SZ, ctypes.POINTER(Launch),
                                      _VP, _SZ, _VP]),
     "ss_server_create": (_I, [ctypes.POINTER(ServerConfig),

@@ -1,6 +1,7 @@
 """Build recipe for the CUDA route library (sm_100a).
 
-Compiles ``csrc/ss_route.cu`` (the route), ``csrc/ss_server.cu`` (the
+Compiles ``csrc/ss_route.cu`` (the route), ``csrc/ss_static.cu`` (its
+zero-allocation form), ``csrc/ss_server.cu`` (the
 serving loop), ``csrc/ss_pack.cu`` (compact mask transfer, host side with
 OpenMP) and ``csrc/ss_image_io.cpp`` (PGM / PNG / BMP / JPEG / TIFF files, zlib) into ``libsparseseam.so`` next to this file with
 nvcc.  The library has a plain C ABI (``include/sparse_seam.h``) and links the
@@ -17,13 +18,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 INCLUDE = os.path.join(ROOT, "include")
 SOURCES = [os.path.join(HERE, "csrc", "ss_route.cu"),
+           os.path.join(HERE, "csrc", "ss_static.cu"),
            os.path.join(HERE, "csrc", "ss_server.cu"),
            os.path.join(HERE, "csrc", "ss_pack.cu"),
            os.path.join(HERE, "csrc", "ss_image_io.cpp")]
 DEPENDS = SOURCES + [
     os.path.join(HERE, "csrc", name)
     for name in ("ss_device.cuh", "ss_tile.cuh", "ss_rowscan.cuh",
-                 "ss_runs.cuh", "ss_internal.h", "ss_pool.hpp")
+                 "ss_runs.cuh", "ss_internal.h", "ss_pool.hpp",
+                 "ss_percentile.hpp")
 ] + [os.path.join(INCLUDE, "sparse_seam.h")]
 LIBRARY = os.path.join(HERE, "libsparseseam.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -54,7 +57,8 @@ def harness_command(output: str) -> list:
     """The command-line harness: host C++ over the C ABI, linked against
     the library next to it (rpath $ORIGIN)."""
     return [
-        nvcc(), *ARCH, "-O2", "-std=c++17", "-I" + INCLUDE, "-o", output,
+        nvcc(), *ARCH, "-O2", "-std=c++17", "-I" + INCLUDE,
+        "-I" + os.path.join(HERE, "csrc"), "-o", output,
         HARNESS_SOURCE, "-L" + HERE, "-lsparseseam",
         "-Xlinker", "-rpath,$ORIGIN",
     ]

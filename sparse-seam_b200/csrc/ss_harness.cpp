@@ -38,6 +38,7 @@
 #include <vector>
 
 #include "sparse_seam.h"
+#include "ss_percentile.hpp"
 
 namespace fs = std::filesystem;
 
@@ -62,15 +63,7 @@ void check_ss(ss_status s, const char* what) {
     }
 }
 
-// Nearest-rank percentile of a sample (the reference's percentile helper
-// sorts and takes element ceil(q * n) - 1).
-double percentile(std::vector<double> v, double q) {
-    if (v.empty()) return 0.0;
-    std::sort(v.begin(), v.end());
-    size_t k = static_cast<size_t>(q * static_cast<double>(v.size()) + 0.999999);
-    k = k == 0 ? 0 : k - 1;
-    return v[std::min(k, v.size() - 1)];
-}
+using ss_harness::percentile;
 
 std::string quote(const std::string& s) {
     std::string out = "\"";

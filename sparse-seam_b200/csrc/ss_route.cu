@@ -430,9 +430,15 @@ __global__ void init_header_kernel(Header* h) {
     h->magic = kMagic;
 }
 
+// A kernel that does nothing: the launch-floor measurement's unit.
+__global__ void empty_kernel() {}
+
 // ---------------------------------------------------------------------------
 // Row-scan kernels (T = 32): NW independent warps per CTA, one tile each.
 // ---------------------------------------------------------------------------
+
+// Items a warp of the persistent row-scan tile pass takes per pop.
+constexpr uint32_t kQueueChunk = 8u;
 
 // Row-scan tile pass: NW independent warps per CTA, one tile each; at most
 // 64 registers per thread, so 32 warps fit on an SM (the shared-memory
@@ -455,17 +461,23 @@ runs_tile_pass_kernel(Source src, Arena a) {
         a.header->route = 1u;
     }
     if constexpr (kPersistent) {
+        // Each pop takes a chunk of consecutive items (one atomic per chunk,
+        // and neighbouring tiles of one image on one warp).
         for (;;) {
-            uint32_t item = 0;
+            uint32_t first = 0;
             if (lane == 0) {
-                item = atomicAdd(&a.header->queue_head, 1u);
+                first = atomicAdd(&a.header->queue_head, kQueueChunk);
             }
-            item = __shfl_sync(~0u, item, 0);
-            if (static_cast<int64_t>(item) >= src.total_tiles) {
+            first = __shfl_sync(~0u, first, 0);
+            if (static_cast<int64_t>(first) >= src.total_tiles) {
                 break;
             }
-            rowscan::tile_pass_runs_warp(sm[warp], src, a, item);
-            __syncwarp();
+            const int64_t end = min(src.total_tiles,
+                                    static_cast<int64_t>(first) + kQueueChunk);
+            for (int64_t item = first; item < end; ++item) {
+                rowscan::tile_pass_runs_warp(sm[warp], src, a, item);
+                __syncwarp();
+            }
         }
     } else {
         const int64_t item = static_cast<int64_t>(blockIdx.x) * NW + warp;
@@ -1046,6 +1058,18 @@ ss_status ss_read_status(void* d_workspace, size_t workspace_bytes,
     return h.error ? static_cast<ss_status>(h.error) : SS_OK;
 }
 
+ss_status ss_empty_launches(int count, int grid, int threads, void* stream) {
+    if (count < 0 || grid <= 0 || threads <= 0 || threads > 1024) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    (void)cudaGetLastError();
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    for (int i = 0; i < count; ++i) {
+        empty_kernel<<<static_cast<unsigned>(grid), threads, 0, st>>>();
+    }
+    return cudaGetLastError() == cudaSuccess ? SS_OK : SS_ERR_CUDA;
+}
+
 ss_status ss_set_kernel_config(int tile, int warps) {
     if (!tile_ok(tile)) {
         return SS_ERR_UNSUPPORTED_TILE;
@@ -1258,88 +1282,6 @@ ss_status ss_extrema_batch_pass(const void* h_plan, const void* d_plan,
     }
     return batch_passes(h_plan, d_plan, plan_bytes, persistent, d_workspace,
                         workspace_bytes, stream, pass);
-}
-
-// ---------------------------------------------------------------------------
-// Zero-allocation form
-// ---------------------------------------------------------------------------
-
-// Some callers cannot allocate device memory: code that runs where the
-// allocator must not be entered (inside another allocator's callback, a
-// latency-critical loop that may not block on cudaMalloc), or a plug-in whose
-// host owns every device allocation.  For them the route's scratch lives in
-// this fixed array instead of a caller-provided workspace.  Every GPU that
-// loads the library holds it until the process exits.
-constexpr size_t kStaticScratchBytes = static_cast<size_t>(32) << 20;
-static __device__ __align__(256) unsigned char
-    g_static_scratch[kStaticScratchBytes];
-
-static std::mutex g_static_mutex;
-static void* g_static_address[256] = {};   // per device, set on first use
-
-ss_status ss_extrema_static_scratch(const uint8_t* d_image, int width,
-                                    int height, int pitch, int tile,
-                                    uint8_t* d_maxima, uint8_t* d_minima,
-                                    int out_pitch, void* stream) {
-    if (!d_image || !d_maxima || !d_minima || width <= 0 || height <= 0 ||
-        pitch < width || out_pitch < width) {
-        return SS_ERR_INVALID_VALUE;
-    }
-    if (!tile_ok(tile)) {
-        return SS_ERR_UNSUPPORTED_TILE;
-    }
-    const int64_t tiles = tiles_of(width, height, tile);
-    size_t needed = 0;
-    if (!workspace_size(tiles, tile, &needed)) {
-        return SS_ERR_TOO_LARGE;
-    }
-    if (needed > kStaticScratchBytes) {
-        return SS_ERR_EXCEEDS_STATIC_SCRATCH;
-    }
-    int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess) {
-        return SS_ERR_CUDA;
-    }
-    if (device < 0 || device >= 256) {
-        return SS_ERR_INVALID_VALUE;
-    }
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    void* scratch = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_static_mutex);
-        if (!g_static_address[device]) {
-            // First use on this device (which is current): the array's
-            // device address, then a full clear and the status header.  The
-            // set-up is waited for, so later calls on any stream see it.
-            void* address = nullptr;
-            if (cudaGetSymbolAddress(&address, g_static_scratch) !=
-                    cudaSuccess ||
-                !address) {
-                return SS_ERR_CUDA;
-            }
-            const ss_status init =
-                ss_workspace_init(address, kStaticScratchBytes, stream);
-            if (init != SS_OK) {
-                return init;
-            }
-            if (cudaStreamSynchronize(st) != cudaSuccess) {
-                return SS_ERR_CUDA;
-            }
-            g_static_address[device] = address;
-        }
-        scratch = g_static_address[device];
-    }
-    // The array keeps the previous call's contents.  What this call needs at
-    // zero: the error word and the seam-pair counters of this geometry.
-    Header* header = static_cast<Header*>(scratch);
-    if (cudaMemsetAsync(&header->error, 0, 2 * sizeof(uint32_t), st) !=
-            cudaSuccess ||
-        cudaMemsetAsync(static_cast<char*>(scratch) + sizeof(Header), 0,
-                        static_cast<size_t>(tiles) * 16, st) != cudaSuccess) {
-        return SS_ERR_CUDA;
-    }
-    return ss_extrema(d_image, width, height, pitch, tile, d_maxima, d_minima,
-                      out_pitch, scratch, kStaticScratchBytes, stream);
 }
 
 // ---------------------------------------------------------------------------

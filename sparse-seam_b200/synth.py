@@ -108,7 +108,6 @@ def ellipse_edt(height: int = 1024, width: int = 1024,
     from scipy import ndimage
     rng = np.random.default_rng(seed)
     mask = np.zeros((height, width), dtype=bool)
-    yy, xx = np.mgrid[0:height, 0:width]
     for _ in range(int(rng.integers(20, 201))):
         cy = rng.uniform(0, height)
         cx = rng.uniform(0, width)
@@ -117,8 +116,8 @@ def ellipse_edt(height: int = 1024, width: int = 1024,
         t = rng.uniform(0, math.pi)
         y0, y1 = int(max(0, cy - 61)), int(min(height, cy + 62))
         x0, x1 = int(max(0, cx - 61)), int(min(width, cx + 62))
-        dy = yy[y0:y1, x0:x1] - cy
-        dx = xx[y0:y1, x0:x1] - cx
+        dy = np.arange(y0, y1)[:, None] - cy
+        dx = np.arange(x0, x1)[None, :] - cx
         u = dx * math.cos(t) + dy * math.sin(t)
         v = -dx * math.sin(t) + dy * math.cos(t)
         mask[y0:y1, x0:x1] |= (u / a) ** 2 + (v / b) ** 2 <= 1.0

@@ -66,12 +66,17 @@ def sha256(path: str) -> str:
 
 def main() -> int:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--reference",
+                        default=os.environ.get("SS_REFERENCE_TREE"),
+                        help="reference tree (default: $SS_REFERENCE_TREE)")
     parser.add_argument(
         "--out",
         default=os.path.join(os.path.dirname(os.path.abspath(__file__)),
                              "oracle_cases.npz"))
     args = parser.parse_args()
+    if not args.reference:
+        parser.error("no reference tree: pass --reference DIR or set "
+                     "SS_REFERENCE_TREE")
 
     names, suites, heights, widths = [], [], [], []
     manifest_max, manifest_min = [], []

@@ -1,6 +1,7 @@
 """The command-line harness (the reference's CLI and CSV columns over the C
 ABI): argument checks on the CPU; a run over image files on the GPU."""
 import csv
+import shutil
 import os
 import subprocess
 
@@ -76,3 +77,17 @@ def test_harness_over_image_files(tmp_path, golden_cases):
     assert (out / "environment.txt").exists()
     got = pkg.read_image(str(out / "masks" / "zz_big_max.pgm"))
     assert np.array_equal(got, want[0])
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_percentiles_interpolate_like_the_reference(tmp_path):
+    """median / p95 columns: linear interpolation at q * (n - 1)
+    (harness/primary/gpu_common_v0_6.cu:86-103), pinned on even-length
+    samples where nearest-rank would differ."""
+    exe = str(tmp_path / "percentile_check")
+    subprocess.check_call([
+        "g++", "-O2", "-std=c++17",
+        "-I" + os.path.join(ROOT, "sparse-seam_b200", "csrc"), "-o", exe,
+        os.path.join(ROOT, "tests", "native", "percentile_check.cpp")])
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0 and out.stdout.strip() == "OK", out.stdout
