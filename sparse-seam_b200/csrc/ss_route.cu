@@ -437,8 +437,8 @@ __global__ void empty_kernel() {}
 // Row-scan kernels (T = 32): NW independent warps per CTA, one tile each.
 // ---------------------------------------------------------------------------
 
-// Items a warp of the persistent row-scan tile pass takes per pop.
-constexpr uint32_t kQueueChunk = 8u;
+// Most items a warp of the persistent row-scan tile pass takes per pop.
+constexpr uint32_t kQueueChunk = 16u;
 
 // Row-scan tile pass: NW independent warps per CTA, one tile each; at most
 // 64 registers per thread, so 32 warps fit on an SM (the shared-memory
@@ -461,19 +461,30 @@ runs_tile_pass_kernel(Source src, Arena a) {
         a.header->route = 1u;
     }
     if constexpr (kPersistent) {
-        // Each pop takes a chunk of consecutive items (one atomic per chunk,
-        // and neighbouring tiles of one image on one warp).
+        // Guided self-scheduling: each pop takes a run of consecutive items
+        // sized to the work left (half of an even share per warp, at most
+        // kQueueChunk), so most items cost no atomic on the shared cursor
+        // and the last ones go out singly, keeping the tail short.
+        const int64_t warps = static_cast<int64_t>(gridDim.x) * NW;
         for (;;) {
             uint32_t first = 0;
+            uint32_t count = 1;
             if (lane == 0) {
-                first = atomicAdd(&a.header->queue_head, kQueueChunk);
+                const int64_t left =
+                    src.total_tiles - static_cast<int64_t>(ld_relaxed(
+                                          &a.header->queue_head));
+                count = static_cast<uint32_t>(
+                    max(int64_t(1), min(static_cast<int64_t>(kQueueChunk),
+                                        left / (2 * warps))));
+                first = atomicAdd(&a.header->queue_head, count);
             }
             first = __shfl_sync(~0u, first, 0);
+            count = __shfl_sync(~0u, count, 0);
             if (static_cast<int64_t>(first) >= src.total_tiles) {
                 break;
             }
             const int64_t end = min(src.total_tiles,
-                                    static_cast<int64_t>(first) + kQueueChunk);
+                                    static_cast<int64_t>(first) + count);
             for (int64_t item = first; item < end; ++item) {
                 rowscan::tile_pass_runs_warp(sm[warp], src, a, item);
                 __syncwarp();

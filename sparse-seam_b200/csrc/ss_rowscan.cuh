@@ -37,6 +37,9 @@ constexpr int kSlots = 4 * T;          // fragment slots per tile
 constexpr int kPendingCap = T * T;     // run-log entries per tile
 constexpr int kHaloW = T + 2;          // staged row: columns x0-1 .. x0+T
 constexpr int kSeamCap = 12 * T;       // seam items per tile
+// Loop runs the tile pass lists in the staged tile's shared memory (the
+// list's 2-byte entries, then three 32-word row arrays, fit its 2316 bytes).
+constexpr int kListCap = 960;
 constexpr uint32_t kDeadRecord = 0xFEu;  // border record of a decided zone
 constexpr uint32_t kNoRecord = 0xFFu;    // border pixel of an inside zone
 // Resolve pass: tiles with at most this many logged runs are written run by

@@ -52,6 +52,7 @@ namespace rowscan {
 
 struct __align__(16) RunSmem {
     uint32_t word[T * T];          // union-find word at each run head
+    uint32_t eq[16];               // seam equality masks (see the tile pass)
     // Tile + halo, -1 outside the image; staged pixel (c, r) at index
     // 1 + r * kHaloW + c, so that tile columns 4k, 4k + 1 share a word.
     int16_t img[kHaloW * kHaloW + 2];
@@ -162,41 +163,58 @@ __device__ __forceinline__ uint32_t run_span(const RunShape& s, uint32_t hs) {
     return (s.q + hs) ^ s.q;
 }
 
+// Bytes 0x00 / 0xFF of the 4 bits of `nib` that sit at bit `shift` of it
+// (the other bits of `nib` are masked off): the product places bit i of the
+// nibble at bit 7 of byte i (copies shifted by 7, 14, 21 and 28 bits do not
+// overlap), and a byte permute that replicates each byte's top bit fills it.
+template <int kShift>
+__device__ __forceinline__ uint32_t expand4(uint32_t nib) {
+    const uint32_t t = (nib & (15u << kShift)) * (0x10204080u >> kShift);
+    uint32_t d;
+    asm("prmt.b32 %0, %1, 0, 0xBA98;" : "=r"(d) : "r"(t));
+    return d;
+}
+
 // Writes the 32 x 32 mask bytes of a full tile from per-row bit masks held
-// by lane = row (`mxb`, `mnb`: 1 = byte 255), `vec` bytes per store (16, 8
-// or 4; rows and bases aligned to it).  Each store instruction covers
-// 32 * vec bytes: 32 / vec lanes per row, vec rows per instruction.
+// by lane = row (`mxb`, `mnb`: 1 = byte 255), VEC bytes per store (16, 8 or
+// 4; rows and bases aligned to it).  Each store instruction covers
+// 32 * VEC bytes: 32 / VEC lanes per row, VEC rows per instruction.
+template <int VEC>
 __device__ __forceinline__ void store_rows(uint8_t* omax, uint8_t* omin,
                                            const TileGeom& g,
                                            int64_t out_pitch, uint32_t mxb,
-                                           uint32_t mnb, int vec) {
+                                           uint32_t mnb) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
-    // vec is 16, 8 or 4: shifts instead of divides.
-    const int lv = 31 - __clz(vec);
-    const int c = lane & ((T >> lv) - 1);
-    const int rr = lane >> (5 - lv);
-    for (int r0 = 0; r0 < T; r0 += vec) {
-        const int r = r0 + rr;
-        const uint32_t bx = __shfl_sync(~0u, mxb, r) >> (c * vec);
-        const uint32_t bn = __shfl_sync(~0u, mnb, r) >> (c * vec);
-        const int64_t o =
-            static_cast<int64_t>(g.y0 + r) * out_pitch + g.x0 + c * vec;
-        if (vec == 16) {
-            *reinterpret_cast<uint4*>(omax + o) =
-                make_uint4(spread4(bx), spread4(bx >> 4), spread4(bx >> 8),
-                           spread4(bx >> 12));
-            *reinterpret_cast<uint4*>(omin + o) =
-                make_uint4(spread4(bn), spread4(bn >> 4), spread4(bn >> 8),
-                           spread4(bn >> 12));
-        } else if (vec == 8) {
-            *reinterpret_cast<uint2*>(omax + o) =
-                make_uint2(spread4(bx), spread4(bx >> 4));
-            *reinterpret_cast<uint2*>(omin + o) =
-                make_uint2(spread4(bn), spread4(bn >> 4));
+    constexpr int kPerRow = T / VEC;
+    const int c = lane % kPerRow;
+    const int rr = lane / kPerRow;
+    const int64_t o =
+        static_cast<int64_t>(g.y0 + rr) * out_pitch + g.x0 + c * VEC;
+    uint8_t* px = omax + o;
+    uint8_t* pn = omin + o;
+    const int64_t step = static_cast<int64_t>(VEC) * out_pitch;
+#pragma unroll
+    for (int r0 = 0; r0 < T; r0 += VEC) {
+        const uint32_t bx = __shfl_sync(~0u, mxb, r0 + rr) >> (c * VEC);
+        const uint32_t bn = __shfl_sync(~0u, mnb, r0 + rr) >> (c * VEC);
+        if constexpr (VEC == 16) {
+            *reinterpret_cast<uint4*>(px) =
+                make_uint4(expand4<0>(bx), expand4<4>(bx), expand4<0>(bx >> 8),
+                           expand4<4>(bx >> 8));
+            *reinterpret_cast<uint4*>(pn) =
+                make_uint4(expand4<0>(bn), expand4<4>(bn), expand4<0>(bn >> 8),
+                           expand4<4>(bn >> 8));
+        } else if constexpr (VEC == 8) {
+            *reinterpret_cast<uint2*>(px) =
+                make_uint2(expand4<0>(bx), expand4<4>(bx));
+            *reinterpret_cast<uint2*>(pn) =
+                make_uint2(expand4<0>(bn), expand4<4>(bn));
         } else {
-            *reinterpret_cast<uint32_t*>(omax + o) = spread4(bx);
-            *reinterpret_cast<uint32_t*>(omin + o) = spread4(bn);
+            *reinterpret_cast<uint32_t*>(px) = expand4<0>(bx);
+            *reinterpret_cast<uint32_t*>(pn) = expand4<0>(bn);
         }
+        px += step;
+        pn += step;
     }
 }
 
@@ -353,6 +371,9 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     // -- row scan: flags, decided pixels, row masks ----------------------------
     const bool col_ok = lane < g.tw;
     uint32_t rL = 0, rGT = 0, rLT = 0, rEU = 0, rEUL = 0, rEUR = 0, rEL = 0;
+    // Bottom seam of a full-height tile: bit x of bEq[d + 1] is pixel
+    // (x, T - 1) equal to pixel (x + d, T) below the tile (d = -1, 0, 1).
+    uint32_t bEq[3] = {0u, 0u, 0u};
     {
         const int16_t* scol = simg + lane;   // staged columns lane .. lane + 2
         int Lp = scol[0];
@@ -410,6 +431,12 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             Lc = Ln;
             Rc = Rn;
         }
+        if (g.th == T) {
+            // The window now holds rows T - 1 (p) and T (c).
+            bEq[0] = __ballot_sync(~0u, vp == Lc);
+            bEq[1] = __ballot_sync(~0u, vp == vc);
+            bEq[2] = __ballot_sync(~0u, vp == Rc);
+        }
     }
 
     __syncwarp();
@@ -439,26 +466,56 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     };
 
     // -- seam masks: border pixels with an equal neighbour outside the tile --
+    // Per side and offset d = -1, 0, 1 along the side, the border pixels
+    // equal to their neighbour across the side at offset d.  Top: row 0's
+    // masks against the halo row (up-left, up, up-right); bottom: the
+    // scan's last step; left: bits 0 of the rows' up-left / left masks and
+    // one comparison with the halo pixel below-left; right: bits 31 of the
+    // up-right masks and two comparisons with the halo column.  Equalities
+    // between two pixels outside the image hold, so every use is restricted
+    // to listed pixels.
     uint32_t sT, sB, sLc, sRc;
     {
-        const int x = lane;
-        const int v0 = px(x, 0);
-        sT = __ballot_sync(~0u, x < g.tw && (px(x - 1, -1) == v0 ||
-                                             px(x, -1) == v0 ||
-                                             px(x + 1, -1) == v0));
-        const int vb = px(x, T - 1);
-        sB = __ballot_sync(~0u, g.th == T && (px(x - 1, T) == vb ||
-                                              px(x, T) == vb ||
-                                              px(x + 1, T) == vb));
+    uint32_t tEq[3], lEq[3], rEq[3];
+    {
         const int y = lane;
+        tEq[0] = __shfl_sync(~0u, rEUL, 0);
+        tEq[1] = __shfl_sync(~0u, rEU, 0);
+        tEq[2] = __shfl_sync(~0u, rEUR, 0);
         const int vl = px(0, y);
-        sLc = __ballot_sync(~0u, y < g.th && (px(-1, y - 1) == vl ||
-                                              px(-1, y) == vl ||
-                                              px(-1, y + 1) == vl));
         const int vr = px(T - 1, y);
-        sRc = __ballot_sync(~0u, g.tw == T && (px(T, y - 1) == vr ||
-                                               px(T, y) == vr ||
-                                               px(T, y + 1) == vr));
+        lEq[0] = __ballot_sync(~0u, (rEUL & 1u) != 0u);
+        lEq[1] = __ballot_sync(~0u, (rEL & 1u) != 0u);
+        lEq[2] = __ballot_sync(~0u, px(-1, y + 1) == vl);
+        rEq[0] = __ballot_sync(~0u, (rEUR >> 31) != 0u);
+        rEq[1] = __ballot_sync(~0u, px(T, y) == vr);
+        rEq[2] = __ballot_sync(~0u, px(T, y + 1) == vr);
+    }
+    if (lane == 0) {
+        // Kept for the seam items at the end, out of the registers.
+        uint4* e4 = reinterpret_cast<uint4*>(sm.eq);
+        e4[0] = make_uint4(tEq[0], tEq[1], tEq[2], bEq[0]);
+        e4[1] = make_uint4(bEq[1], bEq[2], lEq[0], lEq[1]);
+        e4[2] = make_uint4(lEq[2], rEq[0], rEq[1], rEq[2]);
+    }
+    {
+        // Adjacent pixels along each side that are equal (so in one zone
+        // when both are listed): rows 0 and th - 1 (left neighbours),
+        // columns 0 and 31 (upper neighbours).
+        const uint32_t el_t = __shfl_sync(~0u, rEL, 0);
+        const uint32_t el_b = __shfl_sync(~0u, rEL, g.th - 1);
+        const uint32_t eu_l = __ballot_sync(~0u, (rEU & 1u) != 0u);
+        const uint32_t eu_r = __ballot_sync(~0u, (rEU >> 31) != 0u);
+        if (lane == 0) {
+            reinterpret_cast<uint4*>(sm.eq)[3] =
+                make_uint4(el_t, el_b, eu_l, eu_r);
+        }
+    }
+    const uint32_t rows_in = g.th == T ? ~0u : (1u << g.th) - 1u;
+    sT = (tEq[0] | tEq[1] | tEq[2]);
+    sB = (bEq[0] | bEq[1] | bEq[2]);
+    sLc = (lEq[0] | lEq[1] | lEq[2]) & rows_in;
+    sRc = g.tw == T ? (rEq[0] | rEq[1] | rEq[2]) & rows_in : 0u;
     }
 
     // -- per row (lane y): runs, seam and dead pixels --------------------------
@@ -581,24 +638,93 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     uint32_t hmax = c_open & c_dead & c_gt;
     uint32_t hmin = c_open & c_dead & c_lt;
 
+    // -- the loop runs, dealt out evenly -----------------------------------------
+    // The flatten and verdict loops below visit the runs of `loop_heads`.
+    // Row by row (lane = row) they would take as many steps as the busiest
+    // row has runs; instead the runs are listed once in the shared memory of
+    // the staged tile (no longer read) and each step takes the next 32 of
+    // them, whatever their rows.  Entry: row (bits 0-4), head (5-9), own
+    // zone flags (10-12), "undecided" (13).  A tile with more runs than the
+    // list holds (far beyond natural images) keeps the row-by-row order.
+    // The verdicts of the settled runs and the pixels of the logged runs are
+    // collected per row in shared memory (hm_rows, hn_rows, lv_rows).
+    uint16_t* const list = reinterpret_cast<uint16_t*>(sm.img);
+    uint32_t* const hm_rows = reinterpret_cast<uint32_t*>(sm.img) + kListCap / 2;
+    uint32_t* const hn_rows = hm_rows + T;
+    uint32_t* const lv_rows = hn_rows + T;
+    hm_rows[y] = 0u;
+    hn_rows[y] = 0u;
+    lv_rows[y] = 0u;
+    uint32_t n_list = 0;
+    const uint32_t list_at = warp_prefix(__popc(loop_heads), n_list);
+    const bool listed = n_list <= static_cast<uint32_t>(kListCap);
+    if (listed) {
+        uint32_t r = loop_heads;
+        uint32_t k = list_at;
+        while (r) {
+            const int h = __ffs(r) - 1;
+            r &= r - 1u;
+            list[k++] = static_cast<uint16_t>(
+                y | (h << 5) | (((own_gt >> h) & 1u) << 10) |
+                (((own_lt >> h) & 1u) << 11) | (((own_seam >> h) & 1u) << 12) |
+                (((undecided >> h) & 1u) << 13));
+        }
+    }
+    // Steps of the two loops: 32 runs each, or the busiest row's runs.
+    const int steps_all =
+        listed ? static_cast<int>((n_list + 31u) >> 5)
+               : static_cast<int>(__reduce_max_sync(~0u, __popc(loop_heads)));
+    const int steps_und =
+        listed ? steps_all
+               : static_cast<int>(
+                     __reduce_max_sync(~0u, __popc(loop_heads & undecided)));
+    __syncwarp();
+    // The run a lane takes at step `it`: from the list, or the next of its
+    // row's runs in `r` (row order).  Returns false when it has none.
+    auto take = [&](int it, uint32_t& r, int& yy, int& h, uint32_t& own,
+                    bool& und) -> bool {
+        if (listed) {
+            const uint32_t idx = static_cast<uint32_t>(it * 32 + lane);
+            if (idx >= n_list) {
+                return false;
+            }
+            const uint32_t e = list[idx];
+            yy = static_cast<int>(e & 31u);
+            h = static_cast<int>((e >> 5) & 31u);
+            own = (e >> 10) & 7u;
+            und = (e >> 13) & 1u;
+            return true;
+        }
+        if (!r) {
+            return false;
+        }
+        h = __ffs(r) - 1;
+        r &= r - 1u;
+        yy = y;
+        own = ((own_gt >> h) & 1u) * kHasGreater |
+              ((own_lt >> h) & 1u) * kHasSmaller |
+              ((own_seam >> h) & 1u) * kTouchesSeam;
+        und = (undecided >> h) & 1u;
+        return true;
+    };
+
     // -- flatten; zone flags ORed into the roots --------------------------------
     {
         uint32_t r = loop_heads;
-        while (__any_sync(~0u, r != 0u)) {
-            if (r) {
-                const int h = __ffs(r) - 1;
-                r &= r - 1u;
-                const uint32_t own = ((own_gt >> h) & 1u) * kHasGreater |
-                                     ((own_lt >> h) & 1u) * kHasSmaller |
-                                     ((own_seam >> h) & 1u) * kTouchesSeam;
-                const int p = run_word(y, h);
+#pragma unroll 1
+        for (int it = 0; it < steps_all; ++it) {
+            int yy = 0, h = 0;
+            uint32_t own = 0u;
+            bool und = false;
+            if (take(it, r, yy, h, own, und)) {
+                const int p = run_word(yy, h);
                 // The walk keeps the root's word: the flags read from it may
                 // lag other lanes' ORs, which only costs a redundant OR.
                 const uint32_t wp = vw[p];
                 uint32_t wr = wp;
                 int root = p;
 #pragma unroll 1
-                for (int it = 0; it < T * T; ++it) {
+                for (int k = 0; k < T * T; ++k) {
                     const int up = rparent(wr, root);
                     if (up == root) break;
                     root = up;
@@ -618,11 +744,11 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     __syncwarp();
 
     // -- listed pixels: verdicts of settled zones, run log of live zones ------
-    // Per row (lane y): `hmax` / `hmin` collect the heads of the runs of
-    // settled zones whose maxima / minima byte is 255; `vmax` / `vmin` are
-    // those runs' pixels.  A live seam zone gets its record (fragment) when
-    // the loop first meets one of its runs: one lane per root takes the
-    // next number, in the order of the loop's steps and lanes.
+    // `hm_rows` / `hn_rows` collect the heads of the runs of settled zones
+    // whose maxima / minima byte is 255.  A live seam zone gets its record
+    // (fragment) when the loop first meets one of its runs: one lane per
+    // root takes the next number, in the order of the loop's steps and
+    // lanes.
     uint32_t* plog = a.pending + item * kPendingCap;
     int nlog = 0;
     uint32_t live_px = 0u;   // pixels of this lane's logged runs
@@ -633,14 +759,15 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         // one with a smaller neighbour, are in a decided zone: 0 in both
         // masks, nothing to log; only the other runs are visited.
         uint32_t r = loop_heads & undecided;
-        while (__any_sync(~0u, r != 0u)) {
+#pragma unroll 1
+        for (int it = 0; it < steps_und; ++it) {
             bool live = false;
-            int h = 0, root = 0;
+            int h = 0, yy = 0, root = 0;
             uint32_t rec1 = 0u;
-            if (r) {
-                h = __ffs(r) - 1;
-                r &= r - 1u;
-                const int p = run_word(y, h);
+            uint32_t own = 0u;
+            bool und = false;
+            if (take(it, r, yy, h, own, und) && und) {
+                const int p = run_word(yy, h);
                 root = rparent(vw[p], p);
                 const uint32_t w = vw[root];
                 const uint32_t z = (w >> kZoneShift) & 7u;
@@ -648,8 +775,12 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                 if (live) {
                     rec1 = (w >> kRecShift) & 0xFFu;
                 } else {
-                    hmax |= (z & kHasGreater) ? 0u : 1u << h;
-                    hmin |= (z & kHasSmaller) ? 0u : 1u << h;
+                    if (!(z & kHasGreater)) {
+                        atomicOr(hm_rows + yy, 1u << h);
+                    }
+                    if (!(z & kHasSmaller)) {
+                        atomicOr(hn_rows + yy, 1u << h);
+                    }
                 }
             }
             const bool need = live && rec1 == 0u;
@@ -682,14 +813,24 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                 nrec += __popc(leads);
                 __syncwarp();
             }
+            // The run's end, from its row's run ends.
+            const uint32_t ends_yy = __shfl_sync(~0u, ends, yy);
             bool logged = false;
             uint32_t entry = 0u;
             if (live && rec1) {
-                const int e = __ffs(ends & ~((1u << h) - 1u)) - 1;
+                const int e = __ffs(ends_yy & ~((1u << h) - 1u)) - 1;
                 logged = true;
-                entry = pending_entry(static_cast<int>(rec1 - 1u), h, y,
+                entry = pending_entry(static_cast<int>(rec1 - 1u), h, yy,
                                       e - h + 1);
                 live_px += static_cast<uint32_t>(e - h + 1);
+                atomicOr(lv_rows + yy, ((2u << e) - 1u) & ~((1u << h) - 1u));
+                // The run's own head word also carries the record (a root's
+                // already does; other head words have these bits free, and
+                // only this lane touches this run's word).
+                const int p = run_word(yy, h);
+                if (p != root) {
+                    vw[p] |= rec1 << kRecShift;
+                }
             }
             const uint32_t bal = __ballot_sync(~0u, logged);
             if (logged) {
@@ -698,6 +839,10 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             nlog += __popc(bal);
         }
     }
+    __syncwarp();
+    hmax |= hm_rows[y];
+    hmin |= hn_rows[y];
+    const uint32_t live_row = lv_rows[y];   // pixels of this row's logged runs
     const uint32_t vmax = run_span(shape, hmax);
     const uint32_t vmin = run_span(shape, hmin);
     // The tile's logged pixels (a statistic: bits 16-31 of its log count).
@@ -717,8 +862,12 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         if (g.tw < T || g.th < T) {
             vec = 1;
         }
-        if (vec > 1) {
-            store_rows(omax, omin, g, out_pitch, vmax, vmin, vec);
+        if (vec == 16) {
+            store_rows<16>(omax, omin, g, out_pitch, vmax, vmin);
+        } else if (vec == 8) {
+            store_rows<8>(omax, omin, g, out_pitch, vmax, vmin);
+        } else if (vec == 4) {
+            store_rows<4>(omax, omin, g, out_pitch, vmax, vmin);
         } else {
             uint8_t* pmx = omax + static_cast<int64_t>(g.y0) * out_pitch +
                            g.x0 + lane;
@@ -739,99 +888,110 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     }
 
     // -- border records, seam items ---------------------------------------------
+    // Border record of every side pixel: its zone's record if the zone is
+    // live (then one of its runs was logged, and the run's head word holds
+    // the record), else "dead": a pixel equal to a pixel across the seam is
+    // in a zone touching the seam, so it is live or decided.
     uint8_t* border = a.border + item * kSlots;
-    // Record of tile pixel (x, yy) whose row has listed mask `lrow` and run
-    // heads `hrow`.
-    auto record_of = [&](int x, int yy, uint32_t lrow,
-                         uint32_t hrow) -> uint32_t {
-        if (!((lrow >> x) & 1u)) {
-            return kDeadRecord;   // a decided pixel
-        }
-        const int p = run_word(yy, head_of(hrow, x));
-        const int root = rparent(vw[p], p);
-        const uint32_t w = vw[root];
-        const uint32_t z = (w >> kZoneShift) & 7u;
-        if ((z & kDead) == kDead) {
-            return kDeadRecord;
-        }
-        const uint32_t r1 = (w >> kRecShift) & 0xFFu;
-        return r1 ? r1 - 1u : kNoRecord;
+    auto rec_at = [&](int x, int yy, uint32_t hrow) -> uint32_t {
+        const uint32_t w = vw[run_word(yy, head_of(hrow, x))];
+        return ((w >> kRecShift) & 0xFFu) - 1u;
     };
+    const uint32_t live_t = __shfl_sync(~0u, live_row, 0);
+    const uint32_t heads_t = __shfl_sync(~0u, heads, 0);
+    const uint32_t live_b0 = __shfl_sync(~0u, live_row, g.th - 1);
+    const uint32_t heads_b = __shfl_sync(~0u, heads, g.th - 1);
+    const uint32_t live_l = __ballot_sync(~0u, (live_row & 1u) != 0u);
+    const uint32_t live_r0 =
+        __ballot_sync(~0u, ((live_row >> (g.tw - 1)) & 1u) != 0u);
+    const uint32_t bit = 1u << lane;
+    const uint32_t rt = (live_t & bit) ? rec_at(lane, 0, heads_t) : kDeadRecord;
+    const uint32_t rb =
+        (live_b0 & bit) ? rec_at(lane, g.th - 1, heads_b) : kDeadRecord;
+    const uint32_t rl = (live_row & 1u) ? rec_at(0, y, heads) : kDeadRecord;
+    const uint32_t rr = ((live_row >> (g.tw - 1)) & 1u)
+                            ? rec_at(g.tw - 1, y, heads) : kDeadRecord;
+    if (lane < g.tw) {
+        border[lane] = static_cast<uint8_t>(rt);
+        border[T + lane] = static_cast<uint8_t>(rb);
+    }
+    if (lane < g.th) {
+        border[2 * T + lane] = static_cast<uint8_t>(rl);
+        border[3 * T + lane] = static_cast<uint8_t>(rr);
+    }
+    // Seam items: one per equal pair (live pixel here, pixel across the
+    // seam at offset d), except that of a streak of such pairs in one
+    // direction whose pixels here are adjacent and in one zone (so are
+    // their partners, adjacent and equal: one zone in one neighbour tile)
+    // only the first is kept.  Lanes are the positions along the side.
     uint32_t* items = a.seam_items + item * kSeamCap;
     int nitems = 0;
-    // Lanes are consecutive border positions.  When the previous position
-    // emits the same record in the same direction, both pairs join the same
-    // two zones (our two pixels share a record, so a zone and a value; their
-    // partners are 4-adjacent pixels of that value in one neighbour tile, so
-    // one zone there too): only the first pair of such a streak is emitted.
-    auto emit = [&](bool ok_in, uint32_t rec, int dir, int off) {
-        const int key = ok_in ? static_cast<int>(rec | (dir << 8)) : -1;
-        const int prev = __shfl_up_sync(~0u, key, 1);
-        const bool ok = ok_in && !(lane > 0 && prev == key);
-        const uint32_t bal = __ballot_sync(~0u, ok);
-        if (ok) {
-            items[nitems + __popc(bal & lt_mask)] =
+    auto emit = [&](uint32_t m, uint32_t rec, int dir, int off) {
+        if (m & bit) {
+            items[nitems + __popc(m & lt_mask)] =
                 rec | (static_cast<uint32_t>(off) << 8) |
                 (static_cast<uint32_t>(dir) << 16);
         }
-        nitems += __popc(bal);
+        nitems += __popc(m);
     };
+    // Keeps the first pair of every streak: c are the candidate positions,
+    // same the positions whose pixel is in the zone of the previous one.
+    auto firsts = [](uint32_t c, uint32_t same) {
+        return c & ~((c << 1) & same);
+    };
+    uint32_t qT[3], qB[3], qL[3], qR[3], el_t, el_b, eu_l, eu_r;
     {
-        const uint32_t l_top = __shfl_sync(~0u, rL, 0);
-        const uint32_t h_top = __shfl_sync(~0u, heads, 0);
-        const uint32_t l_bot = __shfl_sync(~0u, rL, g.th - 1);
-        const uint32_t h_bot = __shfl_sync(~0u, heads, g.th - 1);
-        const int x = lane;
-        const bool in_row = x < g.tw;
-        const uint32_t rt = in_row ? record_of(x, 0, l_top, h_top) : kNoRecord;
-        const uint32_t rb =
-            in_row ? record_of(x, g.th - 1, l_bot, h_bot) : kNoRecord;
-        if (in_row) {
-            border[x] = static_cast<uint8_t>(rt);
-            border[T + x] = static_cast<uint8_t>(rb);
-        }
-        const bool live_t = rt < static_cast<uint32_t>(kSlots);
-        const bool live_b = rb < static_cast<uint32_t>(kSlots) &&
-                            g.th == T && g.y0 + T < height;
-        const int vt = px(x, 0);
-        const int vb = px(x, T - 1);
-        const bool any_tb = __any_sync(~0u, live_t || live_b);
+        const uint4* e4 = reinterpret_cast<const uint4*>(sm.eq);
+        const uint4 e0 = e4[0], e1 = e4[1], e2 = e4[2], e3 = e4[3];
+        el_t = e3.x;
+        el_b = e3.y;
+        eu_l = e3.z;
+        eu_r = e3.w;
+        qT[0] = e0.x; qT[1] = e0.y; qT[2] = e0.z;
+        qB[0] = e0.w; qB[1] = e1.x; qB[2] = e1.y;
+        qL[0] = e1.z; qL[1] = e1.w; qL[2] = e2.x;
+        qR[0] = e2.y; qR[1] = e2.z; qR[2] = e2.w;
+    }
+    const uint32_t rows_in = g.th == T ? ~0u : (1u << g.th) - 1u;
+    const uint32_t live_b =
+        (g.th == T && g.y0 + T < height) ? live_b0 : 0u;
+    const uint32_t live_r =
+        (g.tw == T && g.x0 + T < width) ? live_r0 : 0u;
+    if (live_t | live_b) {
 #pragma unroll
-        for (int d = -1; d <= 1 && any_tb; ++d) {
-            const int x2 = x + d;
-            const int dir_t = x2 < 0 ? kRelTopLeft
-                                     : (x2 >= T ? kRelTopRight : kRelTop);
-            const int off_t = T + (x2 < 0 ? T - 1 : (x2 >= T ? 0 : x2));
-            emit(live_t && px(x2, -1) == vt, rt, dir_t, off_t);
-            const int dir_b = x2 < 0 ? kRelBottomLeft
-                                     : (x2 >= T ? kRelBottomRight : kRelBottom);
-            const int off_b = x2 < 0 ? T - 1 : (x2 >= T ? 0 : x2);
-            emit(live_b && px(x2, T) == vb, rb, dir_b, off_b);
+        for (int d = -1; d <= 1; ++d) {
+            // The direction changes between positions 0 and 1 (d = -1) or
+            // 30 and 31 (d = 1): a streak does not continue across it.
+            const uint32_t cont = d < 0 ? ~2u : (d > 0 ? 0x7FFFFFFFu : ~0u);
+            const int x2 = lane + d;
+            const int side_off = x2 < 0 ? T - 1 : (x2 >= T ? 0 : x2);
+            if (live_t) {
+                emit(firsts(live_t & qT[d + 1], el_t & cont), rt,
+                     x2 < 0 ? kRelTopLeft : (x2 >= T ? kRelTopRight : kRelTop),
+                     T + side_off);
+            }
+            if (live_b) {
+                emit(firsts(live_b & qB[d + 1], el_b & cont), rb,
+                     x2 < 0 ? kRelBottomLeft
+                            : (x2 >= T ? kRelBottomRight : kRelBottom),
+                     side_off);
+            }
         }
     }
-    {
-        const bool in_col = y < g.th;
-        const uint32_t rl = in_col ? record_of(0, y, rL, heads) : kNoRecord;
-        const uint32_t rr =
-            in_col ? record_of(g.tw - 1, y, rL, heads) : kNoRecord;
-        if (in_col) {
-            border[2 * T + y] = static_cast<uint8_t>(rl);
-            border[3 * T + y] = static_cast<uint8_t>(rr);
-        }
-        const bool live_l = rl < static_cast<uint32_t>(kSlots);
-        const bool live_r = rr < static_cast<uint32_t>(kSlots) &&
-                            g.tw == T && g.x0 + T < width;
-        const int vl = px(0, y);
-        const int vr = px(T - 1, y);
-        const bool any_lr = __any_sync(~0u, live_l || live_r);
+    if (live_l | live_r) {
+        // Partners inside the tile's row band only (the corners belong to
+        // the top and bottom sides).
+        const uint32_t band[3] = {rows_in & ~1u, rows_in, rows_in >> 1};
 #pragma unroll
-        for (int d = -1; d <= 1 && any_lr; ++d) {
-            const int y2 = y + d;
-            const bool inside = y2 >= 0 && y2 < g.th;   // corners: rows above
-            emit(live_l && inside && px(-1, y2) == vl, rl, kRelLeft,
-                 3 * T + y2);
-            emit(live_r && inside && px(T, y2) == vr, rr, kRelRight,
-                 2 * T + y2);
+        for (int d = -1; d <= 1; ++d) {
+            if (live_l) {
+                emit(firsts(live_l & qL[d + 1] & band[d + 1], eu_l), rl,
+                     kRelLeft, 3 * T + y + d);
+            }
+            if (live_r) {
+                emit(firsts(live_r & qR[d + 1] & band[d + 1], eu_r), rr,
+                     kRelRight, 2 * T + y + d);
+            }
         }
     }
     if (lane == 0) {
