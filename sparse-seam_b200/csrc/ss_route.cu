@@ -486,20 +486,64 @@ runs_tile_pass_kernel(Source src, Arena a) {
             const int64_t end = min(src.total_tiles,
                                     static_cast<int64_t>(first) + count);
             for (int64_t item = first; item < end; ++item) {
-                rowscan::tile_pass_runs_warp(sm[warp], src, a, item);
+                rowscan::tile_pass_runs<1>(sm[warp].word, sm[warp].aux,
+                                           nullptr, 0, src, a, item);
                 __syncwarp();
             }
         }
     } else {
         const int64_t item = static_cast<int64_t>(blockIdx.x) * NW + warp;
         if (item < src.total_tiles) {
-            rowscan::tile_pass_runs_warp(sm[warp], src, a, item);
+            rowscan::tile_pass_runs<1>(sm[warp].word, sm[warp].aux, nullptr,
+                                       0, src, a, item);
         }
+    }
+}
+
+// Row-scan tile pass at tile edge 64: one CTA of 4 warps per tile, one warp
+// per 32 x 32 quadrant, at most 64 registers per thread (8 CTAs, 32 warps
+// per SM; 27 KB of shared memory per CTA).
+template <bool kPersistent>
+__global__ void __launch_bounds__(128, 8)
+runs64_tile_pass_kernel(Source src, Arena a) {
+    __shared__ rowscan::RunSmem64 sm;
+    __shared__ uint32_t next_item;
+    const int warp = static_cast<int>(threadIdx.x) >> 5;
+    if (a.header->magic != kMagic) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            raise_error(a.header, kErrUninitialized, 0u);
+        }
+        return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.header->last_tiles = static_cast<uint64_t>(src.total_tiles);
+        a.header->tile = 64u;
+        a.header->route = 1u;
+    }
+    if constexpr (kPersistent) {
+        for (;;) {
+            if (threadIdx.x == 0) {
+                next_item = atomicAdd(&a.header->queue_head, 1u);
+            }
+            __syncthreads();
+            const int64_t item = next_item;
+            __syncthreads();   // every thread has read next_item
+            if (item >= src.total_tiles) {
+                break;
+            }
+            rowscan::tile_pass_runs<4>(sm.word, sm.aux[warp], &sm.cta, warp,
+                                       src, a, item);
+            __syncthreads();
+        }
+    } else {
+        rowscan::tile_pass_runs<4>(sm.word, sm.aux[warp], &sm.cta, warp, src,
+                                   a, blockIdx.x);
     }
 }
 
 // Passes after the row-scan tile pass: one CTA of kLaterWarps warps per
 // group of src.group consecutive tiles.
+template <int TT>
 __global__ void __launch_bounds__(rowscan::kLaterWarps * 32)
 rowscan_seam_pass_kernel(Source src, Arena a) {
     if (a.header->magic != kMagic) {
@@ -508,10 +552,12 @@ rowscan_seam_pass_kernel(Source src, Arena a) {
     const int warp = static_cast<int>(threadIdx.x) >> 5;
     const int64_t first = static_cast<int64_t>(blockIdx.x) * src.group;
     if (first < src.total_tiles) {
-        rowscan::seam_pass_group(src, a, first, warp, rowscan::kLaterWarps);
+        rowscan::seam_pass_group<TT>(src, a, first, warp,
+                                     rowscan::kLaterWarps);
     }
 }
 
+template <int TT>
 __global__ void __launch_bounds__(rowscan::kLaterWarps * 32)
 rowscan_flags_pass_kernel(Source src, Arena a) {
     if (a.header->magic != kMagic) {
@@ -520,14 +566,15 @@ rowscan_flags_pass_kernel(Source src, Arena a) {
     const int warp = static_cast<int>(threadIdx.x) >> 5;
     const int64_t first = static_cast<int64_t>(blockIdx.x) * src.group;
     if (first < src.total_tiles) {
-        rowscan::flags_pass_group(src, a, first, warp, rowscan::kLaterWarps);
+        rowscan::flags_pass_group<TT>(src, a, first, warp,
+                                      rowscan::kLaterWarps);
     }
 }
 
-template <bool kPersistent>
+template <int TT, bool kPersistent>
 __global__ void __launch_bounds__(rowscan::kLaterWarps * 32)
 rowscan_resolve_pass_kernel(Source src, Arena a) {
-    __shared__ rowscan::ResolveSmem sm;
+    __shared__ rowscan::ResolveSmem<TT> sm;
     __shared__ uint32_t next_group;
     const int warp = static_cast<int>(threadIdx.x) >> 5;
     if (a.header->magic != kMagic) {
@@ -545,7 +592,7 @@ rowscan_resolve_pass_kernel(Source src, Arena a) {
             if (first >= src.total_tiles) {
                 break;
             }
-            rowscan::resolve_group(sm, src, a, first, warp,
+            rowscan::resolve_group<TT>(sm, src, a, first, warp,
                                    rowscan::kLaterWarps);
         }
         // The last CTA to finish rewinds both work queues for the next call.
@@ -561,7 +608,7 @@ rowscan_resolve_pass_kernel(Source src, Arena a) {
     } else {
         const int64_t first = static_cast<int64_t>(blockIdx.x) * src.group;
         if (first < src.total_tiles) {
-            rowscan::resolve_group(sm, src, a, first, warp,
+            rowscan::resolve_group<TT>(sm, src, a, first, warp,
                                    rowscan::kLaterWarps);
         }
     }
@@ -609,16 +656,18 @@ static bool layout_for(int64_t tiles, int tile, size_t workspace_bytes,
     off = round_up(off + static_cast<size_t>(slots) * 4);
     L.bits = off;
     off = round_up(off + static_cast<size_t>(slots) * 4);
-    // The row-scan path (T = 32) logs pending runs: at most T * T per tile.
-    const size_t pend = tile == 32 ? static_cast<size_t>(tiles) : 0;
+    // The row-scan kernels (T = 32, 64) log pending runs, at most T * T per
+    // tile, and up to 12 T seam items per tile.
+    const size_t pend = tile >= 32 ? static_cast<size_t>(tiles) : 0;
+    const size_t t2 = static_cast<size_t>(tile) * tile;
     L.pending_count = off;
     off = round_up(off + pend * 4);
     L.pending = off;
-    off = round_up(off + pend * 32 * 32 * 4);
+    off = round_up(off + pend * t2 * 4);
     L.seam_count = off;
     off = round_up(off + pend * 4);
     L.seam_items = off;
-    off = round_up(off + pend * rowscan::kSeamCap * 4);
+    off = round_up(off + pend * 12 * tile * 4);
     L.total = off;
     *out = L;
     return L.total <= workspace_bytes &&
@@ -631,12 +680,13 @@ static bool workspace_size(int64_t tiles, int tile, size_t* bytes) {
         return false;
     }
     const size_t slots = static_cast<size_t>(tiles) * 4 * tile;
-    const size_t pend = tile == 32 ? static_cast<size_t>(tiles) : 0;
+    const size_t pend = tile >= 32 ? static_cast<size_t>(tiles) : 0;
+    const size_t t2 = static_cast<size_t>(tile) * tile;
     const size_t dirty = round_up(static_cast<size_t>(tiles) * 2) +
                          round_up(slots) + 2 * round_up(slots * 4) +
-                         round_up(pend * 4) + round_up(pend * 32 * 32 * 4) +
+                         round_up(pend * 4) + round_up(pend * t2 * 4) +
                          round_up(pend * 4) +
-                         round_up(pend * rowscan::kSeamCap * 4);
+                         round_up(pend * 12 * tile * 4);
     size_t s = round_up((dirty + 512) / 31 * 32 + 512);
     Layout L;
     for (int i = 0; i < 1024 && !layout_for(tiles, tile, s, &L); ++i) {
@@ -691,29 +741,40 @@ struct Config {
             {resolve_pass_kernel<T, NW, false>,                               \
              resolve_pass_kernel<T, NW, true>}, 1, nullptr, 1, nullptr        \
     }
-// Row-scan configurations are listed with warps = -NW (one tile per warp).
+// Row-scan configurations are listed with warps = -NW: at tile edge 32 one
+// tile per warp, NW warps per CTA; at tile edge 64 (-4) one tile per CTA of
+// four quadrant warps.
 #define SS_ROWSCAN(NW)                                                        \
     Config {                                                                  \
         32, -(NW),                                                            \
             {runs_tile_pass_kernel<NW, false>,                                \
              runs_tile_pass_kernel<NW, true>},                                \
-            {rowscan_resolve_pass_kernel<false>,                              \
-             rowscan_resolve_pass_kernel<true>}, NW,                          \
-            rowscan_seam_pass_kernel, 32, rowscan_flags_pass_kernel           \
+            {rowscan_resolve_pass_kernel<32, false>,                          \
+             rowscan_resolve_pass_kernel<32, true>}, NW,                      \
+            rowscan_seam_pass_kernel<32>, 32, rowscan_flags_pass_kernel<32>   \
+    }
+#define SS_ROWSCAN64()                                                        \
+    Config {                                                                  \
+        64, -4,                                                               \
+            {runs64_tile_pass_kernel<false>, runs64_tile_pass_kernel<true>},  \
+            {rowscan_resolve_pass_kernel<64, false>,                          \
+             rowscan_resolve_pass_kernel<64, true>}, 1,                       \
+            rowscan_seam_pass_kernel<64>, 32, rowscan_flags_pass_kernel<64>   \
     }
 
 static const Config kConfigs[] = {
     SS_CONFIG(16, 2), SS_CONFIG(16, 4), SS_CONFIG(16, 8),
     SS_CONFIG(32, 4), SS_CONFIG(32, 8), SS_CONFIG(32, 16),
     SS_CONFIG(64, 8), SS_CONFIG(64, 16),
-    SS_ROWSCAN(2), SS_ROWSCAN(4),
+    SS_ROWSCAN(2), SS_ROWSCAN(4), SS_ROWSCAN64(),
 };
 #undef SS_CONFIG
 #undef SS_ROWSCAN
+#undef SS_ROWSCAN64
 
 // Per tile size, the configuration used by default (index by tile / 16 - 1);
 // negative warps select the row-scan kernels.
-static std::atomic<int> g_default_warps[4] = {{4}, {-2}, {0}, {16}};
+static std::atomic<int> g_default_warps[4] = {{4}, {-2}, {0}, {-4}};
 
 static const Config* find_config(int tile, int warps) {
     for (const Config& c : kConfigs) {
@@ -1038,7 +1099,7 @@ ss_status ss_read_status(void* d_workspace, size_t workspace_bytes,
                 sum += c;
             }
             stats->active_fragments = sum;
-            if (h.route == 1u && h.tile == 32u) {
+            if (h.route == 1u) {
                 // Pixels of the logged runs: bits 16-31 of each tile's
                 // run-log count.
                 std::vector<uint32_t> logs(h.last_tiles);

@@ -26,17 +26,32 @@
 // flag reduction, :583-619; masks from the resolved flags, :477-506.
 #pragma once
 
+#include <type_traits>
+
 #include "ss_device.cuh"
 
 namespace ss {
 
 namespace rowscan {
 
-constexpr int T = 32;
+constexpr int T = 32;                  // the warp's square (a quadrant at
+                                       //   tile edge 64)
 constexpr int kSlots = 4 * T;          // fragment slots per tile
 constexpr int kPendingCap = T * T;     // run-log entries per tile
 constexpr int kHaloW = T + 2;          // staged row: columns x0-1 .. x0+T
 constexpr int kSeamCap = 12 * T;       // seam items per tile
+
+// Per tile edge TT (32, or 64 = 2 x 2 warp squares): fragment slots (4 TT,
+// the reference's SLOTS_PER_TILE), run-log entries and seam items per tile,
+// and the row-mask type of the resolve pass.
+template <int TT>
+struct Edge {
+    static constexpr int kSlots = 4 * TT;
+    static constexpr int kPendingCap = TT * TT;
+    static constexpr int kSeamCap = 12 * TT;
+    using Row = typename std::conditional<TT == 64, unsigned long long,
+                                          uint32_t>::type;
+};
 // Loop runs the tile pass lists in the staged tile's shared memory (the
 // list's 2-byte entries, then three 32-word row arrays, fit its 2316 bytes).
 constexpr int kListCap = 960;
@@ -46,11 +61,13 @@ constexpr uint32_t kNoRecord = 0xFFu;    // border pixel of an inside zone
 // run; denser tiles row by row.
 constexpr uint32_t kSparseRuns = 16u;
 
-// Union-find word of a run head in the tile pass: bits 0-9 parent, 10-12
-// zone flags (at roots), 13-20 record + 1 (at roots of live seam zones).
-constexpr uint32_t kParMask = 0x3FFu;
-constexpr int kZoneShift = 10;
-constexpr int kRecShift = 13;
+// Union-find word of a run head in the tile pass: bits 0-11 parent (XOR
+// the word's own index, so an all-zero word is a root), 12-14 zone flags
+// (at roots), 15-22 record + 1 (at roots of live seam zones, and at the
+// head words of their logged runs).  Indices reach 4095 at tile edge 64.
+constexpr uint32_t kParMask = 0xFFFu;
+constexpr int kZoneShift = 12;
+constexpr int kRecShift = 15;
 constexpr uint32_t kDead = kHasGreater | kHasSmaller;
 
 // Seam item of a tile: bits 0-7 own record, 8-14 the neighbour's border
@@ -68,6 +85,7 @@ struct TileGeom {
     int x0, y0, tw, th;
 };
 
+template <int TT = T>
 __device__ __forceinline__ TileGeom tile_geom(const PlanImage& job,
                                               int64_t local) {
     TileGeom g;
@@ -77,10 +95,10 @@ __device__ __forceinline__ TileGeom tile_geom(const PlanImage& job,
     const uint32_t n = static_cast<uint32_t>(job.tiles_x);
     const int ty = static_cast<int>(l / n);
     const int tx = static_cast<int>(l - static_cast<uint32_t>(ty) * n);
-    g.x0 = tx * T;
-    g.y0 = ty * T;
-    g.tw = min(T, job.width - g.x0);
-    g.th = min(T, job.height - g.y0);
+    g.x0 = tx * TT;
+    g.y0 = ty * TT;
+    g.tw = min(TT, job.width - g.x0);
+    g.th = min(TT, job.height - g.y0);
     return g;
 }
 
@@ -147,9 +165,12 @@ __device__ __forceinline__ int64_t neighbour_tile(int64_t g, int dir,
 // `src.group` consecutive tiles (lane = tile of the group); the group's work
 // is flattened and its 32-wide steps are dealt out to the warps, so a group
 // of dense tiles is shared by all the CTA's warps.
+template <int TT>
 __device__ __forceinline__ void seam_pass_group(const Source& src,
                                                 const Arena& a, int64_t first,
                                                 int warp, int nwarps) {
+    constexpr int kSlots = Edge<TT>::kSlots;
+    constexpr int kSeamCap = Edge<TT>::kSeamCap;
     const int lane = static_cast<int>(threadIdx.x) & 31;
     const int64_t tile = first + lane;
     const bool valid = lane < src.group && tile < src.total_tiles;
@@ -179,7 +200,7 @@ __device__ __forceinline__ void seam_pass_group(const Source& src,
         if (f < total) {
             const uint32_t it = __ldcg(a.seam_items + g * kSeamCap + j);
             const uint32_t rec = it & 0xFFu;
-            const int off = static_cast<int>((it >> 8) & 0x7Fu);
+            const int off = static_cast<int>((it >> 8) & 0xFFu);
             const int dir = static_cast<int>((it >> 16) & 7u);
             const int64_t ng = neighbour_tile(g, dir, tx);
             if (rec >= static_cast<uint32_t>(kSlots) || ng < 0 ||
@@ -223,9 +244,11 @@ __device__ __forceinline__ void seam_pass_group(const Source& src,
 // fragment ORs its flags (its zone's flags and the "decided neighbour across
 // a seam" marks of the seam pass) into its component's root.  The kernel
 // boundaries order it after every link and before every read of a root.
+template <int TT>
 __device__ __forceinline__ void flags_pass_group(const Source& src,
                                                  const Arena& a, int64_t first,
                                                  int warp, int nwarps) {
+    constexpr int kSlots = Edge<TT>::kSlots;
     const int lane = static_cast<int>(threadIdx.x) & 31;
     const int64_t tile = first + lane;
     const bool valid = lane < src.group && tile < src.total_tiles;
@@ -267,8 +290,11 @@ __device__ __forceinline__ uint32_t spread4(uint32_t bits) {
 // Warps per CTA of the seam, flags and resolve passes.
 constexpr int kLaterWarps = 8;
 
+template <int TT>
 struct __align__(16) ResolveSmem {
-    uint8_t final_flags[32][kSlots];   // the group's fragments' verdicts
+    using Row = typename Edge<TT>::Row;
+    uint8_t final_flags[32][Edge<TT>::kSlots];  // the group's fragments'
+                                                //   verdicts
     uint8_t* maxima[32];
     uint8_t* minima[32];
     int64_t out_origin[32];   // offset of the tile's pixel (0, 0)
@@ -277,9 +303,9 @@ struct __align__(16) ResolveSmem {
     int16_t th[32];
     // Per warp, one dense tile at a time: logged pixels per row, and those
     // whose maxima / minima byte is 255.
-    uint32_t live[kLaterWarps][T];
-    uint32_t vmax[kLaterWarps][T];
-    uint32_t vmin[kLaterWarps][T];
+    Row live[kLaterWarps][TT];
+    Row vmax[kLaterWarps][TT];
+    Row vmin[kLaterWarps][TT];
     uint32_t flipped;         // tiles (bits of the group) with a verdict
                               //   other than their tile-local one
 };
@@ -295,24 +321,25 @@ __device__ __forceinline__ uint32_t merge4(uint32_t cur, uint32_t live,
     return (cur & ~m) | (spread4(verdict) & m);
 }
 
+template <int TT, typename Row>
 __device__ __forceinline__ void merge_rows(uint8_t* omax, uint8_t* omin,
-                                           int64_t pitch,
-                                           const uint32_t* live,
-                                           const uint32_t* vmax,
-                                           const uint32_t* vmin, int vec) {
+                                           int64_t pitch, const Row* live,
+                                           const Row* vmax, const Row* vmin,
+                                           int vec) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
-    const int per_row = T / vec;
+    const int per_row = TT / vec;
     const int c = lane % per_row;
     const int rr = lane / per_row;
     const uint32_t full = (vec == 16) ? 0xFFFFu : (vec == 8) ? 0xFFu : 0xFu;
-    for (int r0 = 0; r0 < T; r0 += vec) {
+    for (int r0 = 0; r0 < TT; r0 += 32 / per_row) {
         const int r = r0 + rr;
-        const uint32_t lv = (live[r] >> (c * vec)) & full;
+        const uint32_t lv =
+            static_cast<uint32_t>(live[r] >> (c * vec)) & full;
         if (lv == 0u) {
             continue;
         }
-        const uint32_t bx = vmax[r] >> (c * vec);
-        const uint32_t bn = vmin[r] >> (c * vec);
+        const uint32_t bx = static_cast<uint32_t>(vmax[r] >> (c * vec));
+        const uint32_t bn = static_cast<uint32_t>(vmin[r] >> (c * vec));
         const int64_t o = static_cast<int64_t>(r) * pitch + c * vec;
         const bool all = lv == full;
         if (vec == 16) {
@@ -344,10 +371,14 @@ __device__ __forceinline__ void merge_rows(uint8_t* omax, uint8_t* omin,
 
 // Called by every warp of the CTA with the same `first`; contains
 // __syncthreads, so all of the CTA's threads must call it.
-__device__ __forceinline__ void resolve_group(ResolveSmem& sm,
+template <int TT>
+__device__ __forceinline__ void resolve_group(ResolveSmem<TT>& sm,
                                               const Source& src,
                                               const Arena& a, int64_t first,
                                               int warp, int nwarps) {
+    using Row = typename Edge<TT>::Row;
+    constexpr int kSlots = Edge<TT>::kSlots;
+    constexpr int kPendingCap = Edge<TT>::kPendingCap;
     const int lane = static_cast<int>(threadIdx.x) & 31;
     const int64_t tile = first + lane;
     const bool valid = lane < src.group && tile < src.total_tiles;
@@ -368,7 +399,7 @@ __device__ __forceinline__ void resolve_group(ResolveSmem& sm,
     uint32_t err = 0;
     if (warp == 0 && n) {
         const PlanImage job = load_job(src, tile);
-        const TileGeom g = tile_geom(job, tile - job.tile_base);
+        const TileGeom g = tile_geom<TT>(job, tile - job.tile_base);
         sm.maxima[lane] = job.maxima;
         sm.minima[lane] = job.minima;
         sm.out_origin[lane] =
@@ -456,9 +487,9 @@ __device__ __forceinline__ void resolve_group(ResolveSmem& sm,
     // time: their pixels and verdicts as row masks, then the tile's rows
     // rewritten (logged bytes replaced, the others kept).
     const uint32_t dense = __ballot_sync(~0u, n > kSparseRuns);
-    uint32_t* live_rows = sm.live[warp];
-    uint32_t* vmax_rows = sm.vmax[warp];
-    uint32_t* vmin_rows = sm.vmin[warp];
+    Row* live_rows = sm.live[warp];
+    Row* vmax_rows = sm.vmax[warp];
+    Row* vmin_rows = sm.vmin[warp];
     int rank = 0;
     for (uint32_t d = dense; d; d &= d - 1u, ++rank) {
         if (rank % nwarps != warp) {
@@ -467,9 +498,11 @@ __device__ __forceinline__ void resolve_group(ResolveSmem& sm,
         const int t = __ffs(d) - 1;
         const uint32_t nt = __shfl_sync(~0u, n, t);
         const uint32_t kt = __shfl_sync(~0u, k, t);
-        live_rows[lane] = 0u;
-        vmax_rows[lane] = 0u;
-        vmin_rows[lane] = 0u;
+        for (int r = lane; r < TT; r += 32) {
+            live_rows[r] = 0u;
+            vmax_rows[r] = 0u;
+            vmin_rows[r] = 0u;
+        }
         __syncwarp();
         const int tw = sm.tw[t];
         const int th = sm.th[t];
@@ -485,7 +518,8 @@ __device__ __forceinline__ void resolve_group(ResolveSmem& sm,
                 continue;
             }
             const uint32_t fl = sm.final_flags[t][rec];
-            const uint32_t R = ((2u << (x + n_px - 1)) - 1u) & ~((1u << x) - 1u);
+            const Row R = ((Row(2) << (x + n_px - 1)) - Row(1)) &
+                          ~((Row(1) << x) - Row(1));
             atomicOr(&live_rows[y], R);
             if (!(fl & kHasGreater)) {
                 atomicOr(&vmax_rows[y], R);
@@ -503,18 +537,20 @@ __device__ __forceinline__ void resolve_group(ResolveSmem& sm,
                                static_cast<uint64_t>(pitch);
         int vec = (align & 15u) == 0 ? 16 : (align & 7u) == 0 ? 8
                 : (align & 3u) == 0 ? 4 : 1;
-        if (tw < T || th < T) {
+        if (tw < TT || th < TT) {
             vec = 1;
         }
         if (vec > 1) {
-            merge_rows(omax, omin, pitch, live_rows, vmax_rows, vmin_rows,
-                       vec);
+            merge_rows<TT>(omax, omin, pitch, live_rows, vmax_rows, vmin_rows,
+                           vec);
         } else {
             for (int r = 0; r < th; ++r) {
-                if ((live_rows[r] >> lane) & 1u) {
-                    const int64_t o = static_cast<int64_t>(r) * pitch + lane;
-                    omax[o] = ((vmax_rows[r] >> lane) & 1u) ? 255 : 0;
-                    omin[o] = ((vmin_rows[r] >> lane) & 1u) ? 255 : 0;
+                for (int x = lane; x < TT; x += 32) {
+                    if ((live_rows[r] >> x) & 1u) {
+                        const int64_t o = static_cast<int64_t>(r) * pitch + x;
+                        omax[o] = ((vmax_rows[r] >> x) & 1u) ? 255 : 0;
+                        omin[o] = ((vmin_rows[r] >> x) & 1u) ? 255 : 0;
+                    }
                 }
             }
         }

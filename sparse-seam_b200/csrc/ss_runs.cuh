@@ -50,12 +50,34 @@ namespace ss {
 
 namespace rowscan {
 
+// Per warp (one 32 x 32 square): the seam equality masks kept for the end
+// of the pass, and the staged square (its image pixels + halo, -1 outside
+// the image; staged pixel (c, r) at index 1 + r * kHaloW + c, so that
+// columns 4k, 4k + 1 share a word), later reused for the run list.
+struct __align__(16) RunAux {
+    uint32_t eq[16];
+    int16_t img[kHaloW * kHaloW + 2];
+};
+
+// Tile edge 32: one warp per tile, its own words.
 struct __align__(16) RunSmem {
     uint32_t word[T * T];          // union-find word at each run head
-    uint32_t eq[16];               // seam equality masks (see the tile pass)
-    // Tile + halo, -1 outside the image; staged pixel (c, r) at index
-    // 1 + r * kHaloW + c, so that tile columns 4k, 4k + 1 share a word.
-    int16_t img[kHaloW * kHaloW + 2];
+    RunAux aux;
+};
+
+// Tile edge 64: four warps per tile, one per 32 x 32 quadrant (q = 2 qy +
+// qx), sharing one union-find over the quadrants' run heads (quadrant q's
+// words at q * 1024 + ...), and the tile's counters.
+struct __align__(16) RunCta {
+    uint32_t lmask[4][T];          // listed pixels per quadrant row
+    uint32_t hmask[4][T];          // run heads per quadrant row
+    uint32_t nrec, nlog, nitems, logged_px;
+};
+
+struct __align__(16) RunSmem64 {
+    uint32_t word[4 * T * T];
+    RunAux aux[4];
+    RunCta cta;
 };
 
 // Run-head words store the parent as (parent XOR self) in bits 0-9, so an
@@ -69,11 +91,14 @@ __device__ __forceinline__ uint32_t with_parent(uint32_t w, int x, int p) {
 }
 
 // Find with path halving (used while linking: a non-root word changes only
-// in its parent bits, and halving writes an ancestor).
+// in its parent bits, and halving writes an ancestor).  Walks are bounded by
+// the number of words of a tile.
+constexpr int kWalkBound = 4 * T * T;
+
 __device__ __forceinline__ int rfind(volatile uint32_t* w, int x,
                                      uint32_t& err) {
 #pragma unroll 1
-    for (int it = 0; it < T * T; ++it) {
+    for (int it = 0; it < kWalkBound; ++it) {
         const uint32_t wx = w[x];
         const int p = rparent(wx, x);
         if (p == x) {
@@ -95,7 +120,7 @@ __device__ __forceinline__ void runion(uint32_t* w_, int a, int b,
                                        uint32_t& err) {
     volatile uint32_t* w = w_;
 #pragma unroll 1
-    for (int it = 0; it < 4 * T * T; ++it) {
+    for (int it = 0; it < 4 * kWalkBound; ++it) {
         a = rfind(w, a, err);
         b = rfind(w, b, err);
         if (a == b || err) {
@@ -218,16 +243,56 @@ __device__ __forceinline__ void store_rows(uint8_t* omax, uint8_t* omin,
     }
 }
 
-__device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
-                                                    const Source& src,
-                                                    const Arena& a,
-                                                    int64_t item) {
+// The tile pass over one tile.  Q = 1: tile edge 32, the calling warp
+// labels the whole tile, `words` are its own 1024 union-find words and `cta`
+// is unused.  Q = 4: tile edge 64, the calling warp (q = 2 qy + qx) labels
+// quadrant q of the tile, `words` are the CTA's 4096 words; every warp of
+// the CTA calls this with the same item (it holds __syncthreads).  The
+// quadrants' zones are joined in the shared union-find across the inner
+// sides, so fragments, records, border records, seam items and the run log
+// belong to the 64 x 64 tile.
+template <int Q>
+__device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
+                                               RunCta* cta, int q,
+                                               const Source& src,
+                                               const Arena& a,
+                                               int64_t item) {
+    constexpr int TT = Q == 4 ? 2 * T : T;
+    constexpr int kSlotsT = Edge<TT>::kSlots;
+    constexpr int kPendingT = Edge<TT>::kPendingCap;
+    constexpr int kSeamT = Edge<TT>::kSeamCap;
     const int lane = static_cast<int>(threadIdx.x) & 31;
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint32_t err = 0;
+    const int wb = q * T * T;          // this warp's first word
+    uint32_t* const W = words + wb;
+    const int qx = q & 1;
+    const int qy = q >> 1;
 
     const PlanImage job = load_job(src, item);
-    const TileGeom g = tile_geom(job, item - job.tile_base);
+    const TileGeom tg = tile_geom<TT>(job, item - job.tile_base);
+    // This warp's square: the tile, or its quadrant (possibly empty).
+    TileGeom g = tg;
+    if constexpr (Q == 4) {
+        g.x0 = tg.x0 + T * qx;
+        g.y0 = tg.y0 + T * qy;
+        g.tw = max(0, min(T, tg.tw - T * qx));
+        g.th = max(0, min(T, tg.th - T * qy));
+        if (threadIdx.x == 0) {
+            cta->nrec = 0u;
+            cta->nlog = 0u;
+            cta->nitems = 0u;
+            cta->logged_px = 0u;
+        }
+    }
+    const bool two_cols = Q == 4 && tg.tw > T;
+    const bool two_rows = Q == 4 && tg.th > T;
+    // Which sides of the square are sides of the tile (the others face
+    // another quadrant).
+    const bool ext_t = Q == 1 || qy == 0;
+    const bool ext_b = Q == 1 || qy == 1 || !two_rows;
+    const bool ext_l = Q == 1 || qx == 0;
+    const bool ext_r = Q == 1 || qx == 1 || !two_cols;
     const uint8_t* __restrict__ img = job.image;
     const int64_t pitch = job.pitch;
     const int width = job.width;
@@ -235,7 +300,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     const int64_t out_pitch = job.out_pitch;
     uint8_t* __restrict__ omax = job.maxima;
     uint8_t* __restrict__ omin = job.minima;
-    int16_t* const simg = sm.img + 1;
+    int16_t* const simg = ax.img + 1;
 
     // -- prologue: stage the tile and its halo; zero the words --------------
     // Staged row r holds image row y0 - 1 + r, staged column c image column
@@ -245,9 +310,9 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         // table in the (not yet used) union-find words, built before the
         // loads so that it does not hold registers while they are in flight.
         const bool quantise = levels_active(job.levels);
-        const uint8_t* lut = reinterpret_cast<const uint8_t*>(sm.word);
+        const uint8_t* lut = reinterpret_cast<const uint8_t*>(W);
         if (quantise) {
-            uint8_t* t8 = reinterpret_cast<uint8_t*>(sm.word);
+            uint8_t* t8 = reinterpret_cast<uint8_t*>(W);
 #pragma unroll 1
             for (int k = 0; k < 8; ++k) {
                 const int v = k * 32 + lane;
@@ -261,9 +326,11 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         const int xr = g.x0 + T;
         const int gy0 = g.y0 - 1 + lane;
         const int gy1 = g.y0 + 31 + lane;
-        const bool ok0 =
+        // (An empty quadrant, beyond the image, loads nothing.)
+        const bool any = g.tw > 0 && g.th > 0;
+        const bool ok0 = any &&
             static_cast<unsigned>(gy0) < static_cast<unsigned>(height);
-        const bool ok1 = lane < 2 && static_cast<unsigned>(gy1) <
+        const bool ok1 = any && lane < 2 && static_cast<unsigned>(gy1) <
                                          static_cast<unsigned>(height);
         auto load_halo = [&](int& hl0, int& hr0, int& hl1, int& hr1) {
             hl0 = (xl >= 0 && ok0)
@@ -295,6 +362,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         // pairs (tile columns 4k, 4k + 1 sit on a 4-byte boundary of the
         // staged rows).
         const bool word_rows =
+            g.tw > 0 && g.th > 0 &&
             !quantise && g.x0 > 0 && g.y0 > 0 && g.x0 + T < width &&
             g.y0 + T < height &&
             ((reinterpret_cast<uintptr_t>(img) |
@@ -360,7 +428,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         __syncwarp();
         // Words 0..255 first carry the row masks of the scan and are
         // cleared after it.
-        uint4* w4 = reinterpret_cast<uint4*>(sm.word);
+        uint4* w4 = reinterpret_cast<uint4*>(W);
 #pragma unroll
         for (int k = 2; k < T * T / 128; ++k) {
             w4[k * 32 + lane] = make_uint4(0u, 0u, 0u, 0u);
@@ -416,7 +484,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             const uint32_t bEL = __ballot_sync(~0u, vc == Lc);
             if (lane == 0) {
                 // Row y's masks, picked up by lane y after the scan.
-                uint4* slot = reinterpret_cast<uint4*>(sm.word + 8 * y);
+                uint4* slot = reinterpret_cast<uint4*>(W + 8 * y);
                 slot[0] = make_uint4(bG, bS, bEU, bEUL);
                 slot[1] = make_uint4(bEUR, bEL, 0u, 0u);
             }
@@ -443,7 +511,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     {
         // Lane y takes row y's masks (rows beyond the tile stay 0) and clears
         // the words for the union-find.
-        uint4* slot = reinterpret_cast<uint4*>(sm.word + 8 * lane);
+        uint4* slot = reinterpret_cast<uint4*>(W + 8 * lane);
         if (lane < g.th) {
             const uint4 m0 = slot[0];
             const uint4 m1 = slot[1];
@@ -493,7 +561,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     }
     if (lane == 0) {
         // Kept for the seam items at the end, out of the registers.
-        uint4* e4 = reinterpret_cast<uint4*>(sm.eq);
+        uint4* e4 = reinterpret_cast<uint4*>(ax.eq);
         e4[0] = make_uint4(tEq[0], tEq[1], tEq[2], bEq[0]);
         e4[1] = make_uint4(bEq[1], bEq[2], lEq[0], lEq[1]);
         e4[2] = make_uint4(lEq[2], rEq[0], rEq[1], rEq[2]);
@@ -507,15 +575,16 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         const uint32_t eu_l = __ballot_sync(~0u, (rEU & 1u) != 0u);
         const uint32_t eu_r = __ballot_sync(~0u, (rEU >> 31) != 0u);
         if (lane == 0) {
-            reinterpret_cast<uint4*>(sm.eq)[3] =
+            reinterpret_cast<uint4*>(ax.eq)[3] =
                 make_uint4(el_t, el_b, eu_l, eu_r);
         }
     }
     const uint32_t rows_in = g.th == T ? ~0u : (1u << g.th) - 1u;
-    sT = (tEq[0] | tEq[1] | tEq[2]);
-    sB = (bEq[0] | bEq[1] | bEq[2]);
-    sLc = (lEq[0] | lEq[1] | lEq[2]) & rows_in;
-    sRc = g.tw == T ? (rEq[0] | rEq[1] | rEq[2]) & rows_in : 0u;
+    // Only the tile's own sides are seams.
+    sT = ext_t ? (tEq[0] | tEq[1] | tEq[2]) : 0u;
+    sB = ext_b ? (bEq[0] | bEq[1] | bEq[2]) : 0u;
+    sLc = ext_l ? (lEq[0] | lEq[1] | lEq[2]) & rows_in : 0u;
+    sRc = (ext_r && g.tw == T) ? (rEq[0] | rEq[1] | rEq[2]) & rows_in : 0u;
     }
 
     // -- per row (lane y): runs, seam and dead pixels --------------------------
@@ -548,7 +617,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     dead &= rL;
 
     // -- links: one union per contact of equal runs in rows y - 1 and y -------
-    volatile uint32_t* vw = sm.word;
+    volatile uint32_t* vw = words;
     uint32_t linked = 0u;   // pixels of this row where a union touches a run
     {
         uint32_t headsm1 = __shfl_up_sync(~0u, heads, 1);
@@ -582,9 +651,9 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                 f &= f - 1u;
                 const int xp = ((A >> x) & 1u) ? x
                              : ((B >> x) & 1u) ? x - 1 : x + 1;
-                const int p = run_word(y, head_of(heads, x));
+                const int p = wb + run_word(y, head_of(heads, x));
                 vw[p] = with_parent(0u, p,
-                                    run_word(y - 1, head_of(headsm1, xp)));
+                                    wb + run_word(y - 1, head_of(headsm1, xp)));
             }
         }
         __syncwarp();
@@ -597,15 +666,15 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             if (rest) {
                 const int x = __ffs(rest) - 1;
                 const uint32_t bit = 1u << x;
-                const int p = run_word(y, head_of(heads, x));
+                const int p = wb + run_word(y, head_of(heads, x));
                 if (rest_ab & bit) {
                     const int xp = ((A >> x) & 1u) ? x : x - 1;
-                    runion(sm.word, p, run_word(y - 1, head_of(headsm1, xp)),
-                           err);
+                    runion(words, p,
+                           wb + run_word(y - 1, head_of(headsm1, xp)), err);
                 }
                 if (rest_c & bit) {
-                    runion(sm.word, p,
-                           run_word(y - 1, head_of(headsm1, x + 1)), err);
+                    runion(words, p,
+                           wb + run_word(y - 1, head_of(headsm1, x + 1)), err);
                 }
                 rest_ab &= ~bit;
                 rest_c &= ~bit;
@@ -613,6 +682,124 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         }
     }
     __syncwarp();
+
+    if constexpr (Q == 4) {
+        // -- the quadrants' inner sides ------------------------------------------
+        // Every pair of equal 8-adjacent pixels of two quadrants: a decided
+        // pixel makes the listed one's zone decided ("dead"); two listed
+        // pixels have their runs united in the shared union-find (one union
+        // per streak of such pairs along a side).  Each quadrant handles its
+        // own pixels; pairs whose other pixel lies outside the tile belong
+        // to the tile's sides.
+        cta->lmask[q][y] = rL;
+        cta->hmask[q][y] = heads;
+        __syncthreads();
+        // Quadrant pq's word of the run holding (pc, pr), and whether that
+        // pixel is listed.
+        auto partner = [&](int pq, int pr, int pc, bool& plisted) -> int {
+            plisted = (cta->lmask[pq][pr] >> pc) & 1u;
+            return plisted ? pq * T * T +
+                                 run_word(pr, head_of(cta->hmask[pq][pr], pc))
+                           : 0;
+        };
+        const uint4* e4 = reinterpret_cast<const uint4*>(ax.eq);
+        const uint4 e0 = e4[0], e1 = e4[1], e2 = e4[2], e3 = e4[3];
+        const uint32_t eqT[3] = {e0.x, e0.y, e0.z};
+        const uint32_t eqB[3] = {e0.w, e1.x, e1.y};
+        const uint32_t eqL[3] = {e1.z, e1.w, e2.x};
+        const uint32_t eqR[3] = {e2.y, e2.z, e2.w};
+        auto firsts_ = [](uint32_t c, uint32_t same) {
+            return c & ~((c << 1) & same);
+        };
+        if (!ext_t || !ext_b) {
+            // Top (row 0 against quadrant row 0's bottom rows) or bottom
+            // (row 31 against quadrant row 1's top rows); lanes = columns.
+            const bool top = !ext_t;
+            const int row = top ? 0 : T - 1;
+            const int prow = top ? T - 1 : 0;
+            const int pbase = top ? 0 : 2;   // the partner quadrant row
+            const uint32_t lrow = __shfl_sync(~0u, rL, row);
+            const uint32_t hrow = __shfl_sync(~0u, heads, row);
+            const uint32_t same = top ? e3.x : e3.y;   // row's left equality
+            const uint32_t* eq = top ? eqT : eqB;
+            uint32_t dd = 0u, ll = 0u;
+#pragma unroll
+            for (int d = -1; d <= 1; ++d) {
+                const int xp = lane + d;
+                int pq = -1, pc = xp;
+                if (xp >= 0 && xp < T) {
+                    pq = pbase + qx;
+                } else if (xp < 0 && qx == 1) {
+                    pq = pbase;
+                    pc = T - 1;
+                } else if (xp >= T && qx == 0 && two_cols) {
+                    pq = pbase + 1;
+                    pc = 0;
+                }
+                const bool cand = pq >= 0 && ((lrow >> lane) & 1u) &&
+                                  ((eq[d + 1] >> lane) & 1u);
+                bool pl = false;
+                const int pw = cand ? partner(pq, prow, pc, pl) : 0;
+                const uint32_t un = __ballot_sync(~0u, cand && pl);
+                dd |= __ballot_sync(~0u, cand && !pl);
+                ll |= un;
+                if ((firsts_(un, same) >> lane) & 1u) {
+                    runion(words, wb + run_word(row, head_of(hrow, lane)), pw,
+                           err);
+                }
+            }
+            if (y == row) {
+                dead |= dd;
+                linked |= ll;
+            }
+        }
+        if (!ext_l || !ext_r) {
+            // Left (column 0 against quadrant column 0's right column) or
+            // right (column 31 against column 1's left column); lanes = rows.
+            const bool left = !ext_l;
+            const int col = left ? 0 : T - 1;
+            const int pcol = left ? T - 1 : 0;
+            const int pside = left ? 0 : 1;   // the partner quadrant column
+            const uint32_t same = left ? e3.z : e3.w;  // column's up equality
+            const uint32_t* eq = left ? eqL : eqR;
+            const bool mine = (rL >> col) & 1u;
+            uint32_t dd = 0u, ll = 0u;
+#pragma unroll
+            for (int d = -1; d <= 1; ++d) {
+                const int yp = y + d;
+                int pq = -1, pr = yp;
+                if (yp >= 0 && yp < T) {
+                    pq = 2 * qy + pside;
+                } else if (yp < 0 && qy == 1) {
+                    pq = pside;
+                    pr = T - 1;
+                } else if (yp >= T && qy == 0 && two_rows) {
+                    pq = 2 + pside;
+                    pr = 0;
+                }
+                const bool cand = pq >= 0 && mine && ((eq[d + 1] >> y) & 1u);
+                bool pl = false;
+                const int pw = cand ? partner(pq, pr, pcol, pl) : 0;
+                const uint32_t un = __ballot_sync(~0u, cand && pl);
+                dd |= __ballot_sync(~0u, cand && !pl);
+                ll |= un;
+                if ((firsts_(un, same) >> y) & 1u) {
+                    runion(words, wb + run_word(y, head_of(heads, col)), pw,
+                           err);
+                }
+            }
+            const uint32_t bit_c = 1u << col;
+            if ((dd >> y) & 1u) {
+                dead |= bit_c;
+            }
+            if ((ll >> y) & 1u) {
+                linked |= bit_c;
+            }
+        }
+        dead &= rL;
+        // Every union of the tile is in place before any flatten.
+        __syncthreads();
+    }
 
     // -- runs that are zones of their own ---------------------------------------
     // A run that no union touches is a whole zone; unless it touches a seam,
@@ -648,8 +835,8 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     // list holds (far beyond natural images) keeps the row-by-row order.
     // The verdicts of the settled runs and the pixels of the logged runs are
     // collected per row in shared memory (hm_rows, hn_rows, lv_rows).
-    uint16_t* const list = reinterpret_cast<uint16_t*>(sm.img);
-    uint32_t* const hm_rows = reinterpret_cast<uint32_t*>(sm.img) + kListCap / 2;
+    uint16_t* const list = reinterpret_cast<uint16_t*>(ax.img);
+    uint32_t* const hm_rows = reinterpret_cast<uint32_t*>(ax.img) + kListCap / 2;
     uint32_t* const hn_rows = hm_rows + T;
     uint32_t* const lv_rows = hn_rows + T;
     hm_rows[y] = 0u;
@@ -717,14 +904,14 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             uint32_t own = 0u;
             bool und = false;
             if (take(it, r, yy, h, own, und)) {
-                const int p = run_word(yy, h);
+                const int p = wb + run_word(yy, h);
                 // The walk keeps the root's word: the flags read from it may
                 // lag other lanes' ORs, which only costs a redundant OR.
                 const uint32_t wp = vw[p];
                 uint32_t wr = wp;
                 int root = p;
 #pragma unroll 1
-                for (int k = 0; k < T * T; ++k) {
+                for (int k = 0; k < kWalkBound; ++k) {
                     const int up = rparent(wr, root);
                     if (up == root) break;
                     root = up;
@@ -736,12 +923,17 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                 }
                 const uint32_t zf = (wr >> kZoneShift) & 7u;
                 if ((zf & own) != own) {
-                    atomicOr(sm.word + root, own << kZoneShift);
+                    atomicOr(words + root, own << kZoneShift);
                 }
             }
         }
     }
-    __syncwarp();
+    // Zone flags are complete at every root (of any quadrant) from here on.
+    if constexpr (Q == 4) {
+        __syncthreads();
+    } else {
+        __syncwarp();
+    }
 
     // -- listed pixels: verdicts of settled zones, run log of live zones ------
     // `hm_rows` / `hn_rows` collect the heads of the runs of settled zones
@@ -749,12 +941,12 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     // (fragment) when the loop first meets one of its runs: one lane per
     // root takes the next number, in the order of the loop's steps and
     // lanes.
-    uint32_t* plog = a.pending + item * kPendingCap;
+    uint32_t* plog = a.pending + item * kPendingT;
     int nlog = 0;
     uint32_t live_px = 0u;   // pixels of this lane's logged runs
     uint32_t nrec = 0;
-    const int64_t frag_base = item * kSlots;
-    {
+    const int64_t frag_base = item * kSlotsT;
+    if constexpr (Q == 1) {
         // Runs that hold a dead pixel, or both a pixel with a greater and
         // one with a smaller neighbour, are in a decided zone: 0 in both
         // masks, nothing to log; only the other runs are visited.
@@ -767,7 +959,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
             uint32_t own = 0u;
             bool und = false;
             if (take(it, r, yy, h, own, und) && und) {
-                const int p = run_word(yy, h);
+                const int p = wb + run_word(yy, h);
                 root = rparent(vw[p], p);
                 const uint32_t w = vw[root];
                 const uint32_t z = (w >> kZoneShift) & 7u;
@@ -794,7 +986,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                 uint32_t mine = 0u;
                 if (lead) {
                     const uint32_t rec = nrec + __popc(leads & lt_mask);
-                    if (rec < static_cast<uint32_t>(kSlots)) {
+                    if (rec < static_cast<uint32_t>(kSlotsT)) {
                         const uint32_t w = vw[root];
                         vw[root] = w | ((rec + 1u) << kRecShift);
                         const uint32_t z = (w >> kZoneShift) & 3u;
@@ -827,7 +1019,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                 // The run's own head word also carries the record (a root's
                 // already does; other head words have these bits free, and
                 // only this lane touches this run's word).
-                const int p = run_word(yy, h);
+                const int p = wb + run_word(yy, h);
                 if (p != root) {
                     vw[p] |= rec1 << kRecShift;
                 }
@@ -837,6 +1029,98 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
                 plog[nlog + __popc(bal & lt_mask)] = entry;
             }
             nlog += __popc(bal);
+        }
+    } else {
+        // Tile edge 64: a zone's root may lie in another quadrant, met by
+        // another warp, so records go to the roots first (each root is met
+        // once, at its own run; the tile's counter numbers them), then every
+        // run reads its root.
+        {
+            uint32_t r = loop_heads;
+#pragma unroll 1
+            for (int it = 0; it < steps_all; ++it) {
+                int yy = 0, h = 0, p = 0;
+                uint32_t own = 0u, w = 0u;
+                bool und = false;
+                bool live_root = false;
+                if (take(it, r, yy, h, own, und)) {
+                    p = wb + run_word(yy, h);
+                    w = vw[p];
+                    const uint32_t z = (w >> kZoneShift) & 7u;
+                    live_root = rparent(w, p) == p && (z & kTouchesSeam) &&
+                                (z & kDead) != kDead;
+                }
+                const uint32_t roots = __ballot_sync(~0u, live_root);
+                if (roots) {
+                    uint32_t base = 0u;
+                    if (lane == 0) {
+                        base = atomicAdd(&cta->nrec, __popc(roots));
+                    }
+                    base = __shfl_sync(~0u, base, 0);
+                    if (live_root) {
+                        const uint32_t rec = base + __popc(roots & lt_mask);
+                        if (rec < static_cast<uint32_t>(kSlotsT)) {
+                            vw[p] = w | ((rec + 1u) << kRecShift);
+                            const uint32_t z = (w >> kZoneShift) & 3u;
+                            const int64_t gi = frag_base + rec;
+                            a.parent[gi] = static_cast<int32_t>(gi);
+                            a.bits[gi] = z | (z << kLocalShift);
+                        } else {
+                            err = kErrFragmentOverflow;
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        uint32_t r = loop_heads & undecided;
+#pragma unroll 1
+        for (int it = 0; it < steps_und; ++it) {
+            bool logged = false;
+            int h = 0, yy = 0, p = 0, root = 0;
+            uint32_t rec1 = 0u;
+            uint32_t own = 0u;
+            bool und = false;
+            if (take(it, r, yy, h, own, und) && und) {
+                p = wb + run_word(yy, h);
+                root = rparent(vw[p], p);
+                const uint32_t w = vw[root];
+                const uint32_t z = (w >> kZoneShift) & 7u;
+                if ((z & kTouchesSeam) && (z & kDead) != kDead) {
+                    rec1 = (w >> kRecShift) & 0xFFu;
+                    logged = rec1 != 0u;   // 0: the tile ran out of records
+                } else {
+                    if (!(z & kHasGreater)) {
+                        atomicOr(hm_rows + yy, 1u << h);
+                    }
+                    if (!(z & kHasSmaller)) {
+                        atomicOr(hn_rows + yy, 1u << h);
+                    }
+                }
+            }
+            const uint32_t ends_yy = __shfl_sync(~0u, ends, yy);
+            uint32_t entry = 0u;
+            if (logged) {
+                const int e = __ffs(ends_yy & ~((1u << h) - 1u)) - 1;
+                entry = pending_entry(static_cast<int>(rec1 - 1u), T * qx + h,
+                                      T * qy + yy, e - h + 1);
+                live_px += static_cast<uint32_t>(e - h + 1);
+                atomicOr(lv_rows + yy, ((2u << e) - 1u) & ~((1u << h) - 1u));
+                if (p != root) {
+                    vw[p] |= rec1 << kRecShift;
+                }
+            }
+            const uint32_t bal = __ballot_sync(~0u, logged);
+            if (bal) {
+                uint32_t base = 0u;
+                if (lane == 0) {
+                    base = atomicAdd(&cta->nlog, __popc(bal));
+                }
+                base = __shfl_sync(~0u, base, 0);
+                if (logged) {
+                    plog[base + __popc(bal & lt_mask)] = entry;
+                }
+            }
         }
     }
     __syncwarp();
@@ -892,9 +1176,9 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     // live (then one of its runs was logged, and the run's head word holds
     // the record), else "dead": a pixel equal to a pixel across the seam is
     // in a zone touching the seam, so it is live or decided.
-    uint8_t* border = a.border + item * kSlots;
+    uint8_t* border = a.border + item * kSlotsT;
     auto rec_at = [&](int x, int yy, uint32_t hrow) -> uint32_t {
-        const uint32_t w = vw[run_word(yy, head_of(hrow, x))];
+        const uint32_t w = vw[wb + run_word(yy, head_of(hrow, x))];
         return ((w >> kRecShift) & 0xFFu) - 1u;
     };
     const uint32_t live_t = __shfl_sync(~0u, live_row, 0);
@@ -902,33 +1186,54 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     const uint32_t live_b0 = __shfl_sync(~0u, live_row, g.th - 1);
     const uint32_t heads_b = __shfl_sync(~0u, heads, g.th - 1);
     const uint32_t live_l = __ballot_sync(~0u, (live_row & 1u) != 0u);
+    const int last_col = max(g.tw - 1, 0);
     const uint32_t live_r0 =
-        __ballot_sync(~0u, ((live_row >> (g.tw - 1)) & 1u) != 0u);
+        __ballot_sync(~0u, ((live_row >> last_col) & 1u) != 0u);
     const uint32_t bit = 1u << lane;
     const uint32_t rt = (live_t & bit) ? rec_at(lane, 0, heads_t) : kDeadRecord;
     const uint32_t rb =
         (live_b0 & bit) ? rec_at(lane, g.th - 1, heads_b) : kDeadRecord;
     const uint32_t rl = (live_row & 1u) ? rec_at(0, y, heads) : kDeadRecord;
-    const uint32_t rr = ((live_row >> (g.tw - 1)) & 1u)
-                            ? rec_at(g.tw - 1, y, heads) : kDeadRecord;
+    const uint32_t rr = ((live_row >> last_col) & 1u)
+                            ? rec_at(last_col, y, heads) : kDeadRecord;
+    // Border record arrays: top, bottom, left, right, TT each (positions
+    // along the tile's side).
     if (lane < g.tw) {
-        border[lane] = static_cast<uint8_t>(rt);
-        border[T + lane] = static_cast<uint8_t>(rb);
+        if (ext_t) {
+            border[T * qx + lane] = static_cast<uint8_t>(rt);
+        }
+        if (ext_b) {
+            border[TT + T * qx + lane] = static_cast<uint8_t>(rb);
+        }
     }
     if (lane < g.th) {
-        border[2 * T + lane] = static_cast<uint8_t>(rl);
-        border[3 * T + lane] = static_cast<uint8_t>(rr);
+        if (ext_l) {
+            border[2 * TT + T * qy + lane] = static_cast<uint8_t>(rl);
+        }
+        if (ext_r) {
+            border[3 * TT + T * qy + lane] = static_cast<uint8_t>(rr);
+        }
     }
     // Seam items: one per equal pair (live pixel here, pixel across the
     // seam at offset d), except that of a streak of such pairs in one
     // direction whose pixels here are adjacent and in one zone (so are
     // their partners, adjacent and equal: one zone in one neighbour tile)
     // only the first is kept.  Lanes are the positions along the side.
-    uint32_t* items = a.seam_items + item * kSeamCap;
+    uint32_t* items = a.seam_items + item * kSeamT;
     int nitems = 0;
     auto emit = [&](uint32_t m, uint32_t rec, int dir, int off) {
+        if (!m) {
+            return;
+        }
+        uint32_t base = static_cast<uint32_t>(nitems);
+        if constexpr (Q == 4) {
+            if (lane == 0) {
+                base = atomicAdd(&cta->nitems, __popc(m));
+            }
+            base = __shfl_sync(~0u, base, 0);
+        }
         if (m & bit) {
-            items[nitems + __popc(m & lt_mask)] =
+            items[base + __popc(m & lt_mask)] =
                 rec | (static_cast<uint32_t>(off) << 8) |
                 (static_cast<uint32_t>(dir) << 16);
         }
@@ -941,7 +1246,7 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
     };
     uint32_t qT[3], qB[3], qL[3], qR[3], el_t, el_b, eu_l, eu_r;
     {
-        const uint4* e4 = reinterpret_cast<const uint4*>(sm.eq);
+        const uint4* e4 = reinterpret_cast<const uint4*>(ax.eq);
         const uint4 e0 = e4[0], e1 = e4[1], e2 = e4[2], e3 = e4[3];
         el_t = e3.x;
         el_b = e3.y;
@@ -952,53 +1257,80 @@ __device__ __forceinline__ void tile_pass_runs_warp(RunSmem& sm,
         qL[0] = e1.z; qL[1] = e1.w; qL[2] = e2.x;
         qR[0] = e2.y; qR[1] = e2.z; qR[2] = e2.w;
     }
-    const uint32_t rows_in = g.th == T ? ~0u : (1u << g.th) - 1u;
+    // Only the tile's own sides have seam items, and only where a
+    // neighbour tile lies across them.
+    const uint32_t live_tt = ext_t ? live_t : 0u;
+    const uint32_t live_ll = ext_l ? live_l : 0u;
     const uint32_t live_b =
-        (g.th == T && g.y0 + T < height) ? live_b0 : 0u;
+        (ext_b && tg.th == TT && tg.y0 + TT < height) ? live_b0 : 0u;
     const uint32_t live_r =
-        (g.tw == T && g.x0 + T < width) ? live_r0 : 0u;
-    if (live_t | live_b) {
+        (ext_r && tg.tw == TT && tg.x0 + TT < width) ? live_r0 : 0u;
+    if (live_tt | live_b) {
 #pragma unroll
         for (int d = -1; d <= 1; ++d) {
-            // The direction changes between positions 0 and 1 (d = -1) or
-            // 30 and 31 (d = 1): a streak does not continue across it.
-            const uint32_t cont = d < 0 ? ~2u : (d > 0 ? 0x7FFFFFFFu : ~0u);
-            const int x2 = lane + d;
-            const int side_off = x2 < 0 ? T - 1 : (x2 >= T ? 0 : x2);
-            if (live_t) {
-                emit(firsts(live_t & qT[d + 1], el_t & cont), rt,
-                     x2 < 0 ? kRelTopLeft : (x2 >= T ? kRelTopRight : kRelTop),
-                     T + side_off);
+            // The direction changes between tile positions 0 and 1 (d = -1)
+            // or TT - 2 and TT - 1 (d = 1): a streak does not continue
+            // across it.
+            const uint32_t cont =
+                d < 0 ? (qx == 0 ? ~2u : ~0u)
+                      : (d > 0 ? (T * qx + T == TT ? 0x7FFFFFFFu : ~0u)
+                               : ~0u);
+            const int x2 = T * qx + lane + d;
+            const int side_off = x2 < 0 ? TT - 1 : (x2 >= TT ? 0 : x2);
+            if (live_tt) {
+                emit(firsts(live_tt & qT[d + 1], el_t & cont), rt,
+                     x2 < 0 ? kRelTopLeft : (x2 >= TT ? kRelTopRight : kRelTop),
+                     TT + side_off);
             }
             if (live_b) {
                 emit(firsts(live_b & qB[d + 1], el_b & cont), rb,
                      x2 < 0 ? kRelBottomLeft
-                            : (x2 >= T ? kRelBottomRight : kRelBottom),
+                            : (x2 >= TT ? kRelBottomRight : kRelBottom),
                      side_off);
             }
         }
     }
-    if (live_l | live_r) {
+    if (live_ll | live_r) {
         // Partners inside the tile's row band only (the corners belong to
         // the top and bottom sides).
-        const uint32_t band[3] = {rows_in & ~1u, rows_in, rows_in >> 1};
 #pragma unroll
         for (int d = -1; d <= 1; ++d) {
-            if (live_l) {
-                emit(firsts(live_l & qL[d + 1] & band[d + 1], eu_l), rl,
-                     kRelLeft, 3 * T + y + d);
+            // Rows y of this square whose partner row T qy + y + d lies in
+            // 0 .. tile height - 1.
+            const int lo = max(0, -d - T * qy);
+            const int hi = min(T, tg.th - d - T * qy);
+            const uint32_t band =
+                hi > lo ? ((hi >= 32 ? ~0u : (1u << hi) - 1u) & ~((1u << lo) - 1u))
+                        : 0u;
+            if (live_ll) {
+                emit(firsts(live_ll & qL[d + 1] & band, eu_l), rl, kRelLeft,
+                     3 * TT + T * qy + y + d);
             }
             if (live_r) {
-                emit(firsts(live_r & qR[d + 1] & band[d + 1], eu_r), rr,
-                     kRelRight, 2 * T + y + d);
+                emit(firsts(live_r & qR[d + 1] & band, eu_r), rr, kRelRight,
+                     2 * TT + T * qy + y + d);
             }
         }
     }
-    if (lane == 0) {
-        a.fragment_count[item] =
-            static_cast<uint16_t>(min(nrec, static_cast<uint32_t>(kSlots)));
-        a.pending_count[item] = static_cast<uint32_t>(nlog) | (logged_px << 16);
-        a.seam_count[item] = static_cast<uint32_t>(nitems);
+    if constexpr (Q == 1) {
+        if (lane == 0) {
+            a.fragment_count[item] = static_cast<uint16_t>(
+                min(nrec, static_cast<uint32_t>(kSlotsT)));
+            a.pending_count[item] =
+                static_cast<uint32_t>(nlog) | (logged_px << 16);
+            a.seam_count[item] = static_cast<uint32_t>(nitems);
+        }
+    } else {
+        if (lane == 0 && logged_px) {
+            atomicAdd(&cta->logged_px, logged_px);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            a.fragment_count[item] = static_cast<uint16_t>(
+                min(cta->nrec, static_cast<uint32_t>(kSlotsT)));
+            a.pending_count[item] = cta->nlog | (cta->logged_px << 16);
+            a.seam_count[item] = cta->nitems;
+        }
     }
     if (err) {
         raise_error(a.header, err, static_cast<uint32_t>(item));

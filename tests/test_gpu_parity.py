@@ -14,7 +14,8 @@ pytestmark = pytest.mark.gpu
 
 TILES = (16, 32, 64)
 # (tile, kernel configuration): every kernel family the library ships.
-CONFIGS = [(16, 4), (16, 2), (32, -2), (32, -4), (32, 8), (64, 16), (64, 8)]
+CONFIGS = [(16, 4), (16, 2), (32, -2), (32, -4), (32, 8), (64, -4), (64, 16),
+           (64, 8)]
 
 
 @pytest.fixture
@@ -114,8 +115,9 @@ def test_config1_uniform_q16_and_constant():
     assert (got[0] == 255).all() and (got[1] == 255).all()
 
 
-@pytest.mark.parametrize("kernel_config", [(32, -2), (32, -4), (32, 8)],
-                         indirect=True, ids=["rowscan2", "rowscan4", "cta"])
+@pytest.mark.parametrize("kernel_config", [(32, -2), (32, -4), (32, 8), (64, -4)],
+                         indirect=True,
+                         ids=["rowscan2", "rowscan4", "cta", "rowscan64"])
 def test_plateau_and_seam_heavy_families(kernel_config):
     import importlib
     synth = importlib.import_module("sparse-seam_b200.synth")
@@ -207,8 +209,9 @@ def test_uninitialized_workspace_is_reported():
 
 
 @pytest.mark.parametrize("kernel_config", [(32, -2), (32, 8), (16, 4),
-                                           (64, 16)], indirect=True,
-                         ids=["rowscan", "cta32", "cta16", "cta64"])
+                                           (64, 16), (64, -4)], indirect=True,
+                         ids=["rowscan", "cta32", "cta16", "cta64",
+                              "rowscan64"])
 def test_quantisation_fused_into_the_load(kernel_config):
     """ss_extrema_levels on the original image gives the masks of the
     re-quantised image (the reference's rule, applied on the host there)."""
@@ -245,8 +248,9 @@ def test_quantisation_per_image_in_a_batch():
                         f"image {i} levels {levels[i]}")
 
 
-@pytest.mark.parametrize("kernel_config", [(32, -2), (32, -4)], indirect=True,
-                         ids=["rowscan2", "rowscan4"])
+@pytest.mark.parametrize("kernel_config", [(32, -2), (32, -4), (64, -4)],
+                         indirect=True,
+                         ids=["rowscan2", "rowscan4", "rowscan64"])
 def test_every_store_width(kernel_config):
     """Whole-row mask stores and read-merge-writes at 16, 8, 4 and 1 bytes:
     the output pitch (and base) picks the width, the content has dense live
@@ -283,23 +287,26 @@ def test_every_store_width(kernel_config):
             assert (pad == 9).all(), f"{name} pitch {pitch}: wrote padding"
 
 
-def test_seam_statistics():
+@pytest.mark.parametrize("tile", [32, 64])
+def test_seam_statistics(tile):
     """The status's statistics: a constant image is one zone that crosses
     every seam (every pixel waits for the merge), a one-tile image has no
     seam, and a batch's counts are its images' sums."""
     pkg = package()
     flat = torch.full((300, 200), 77, dtype=torch.uint8, device="cuda")
-    small = torch.randint(0, 256, (32, 32), dtype=torch.uint8, device="cuda")
+    small = torch.randint(0, 256, (tile, tile), dtype=torch.uint8,
+                          device="cuda")
     noisy = torch.randint(0, 4, (256, 320), dtype=torch.uint8, device="cuda")
     per = []
     for im in (flat, small, noisy):
         mx, mn = torch.empty_like(im), torch.empty_like(im)
-        plan = pkg.BatchPlan([im], [mx], [mn], tile=32)
+        plan = pkg.BatchPlan([im], [mx], [mn], tile=tile)
         ws = plan.make_workspace()
         plan.run(ws)
         st = ws.read_status()
         per.append(st)
-        assert st.tiles == ((im.shape[0] + 31) // 32) * ((im.shape[1] + 31) // 32)
+        assert st.tiles == ((im.shape[0] + tile - 1) // tile) * \
+            ((im.shape[1] + tile - 1) // tile)
     assert per[0].live_pixels == flat.numel()
     assert per[0].active_fragments == per[0].tiles
     assert per[1].live_pixels == 0 and per[1].active_fragments == 0
@@ -307,7 +314,7 @@ def test_seam_statistics():
     images = [flat, small, noisy]
     maxs = [torch.empty_like(i) for i in images]
     mins = [torch.empty_like(i) for i in images]
-    plan = pkg.BatchPlan(images, maxs, mins, tile=32)
+    plan = pkg.BatchPlan(images, maxs, mins, tile=tile)
     ws = plan.make_workspace()
     plan.run(ws)
     st = ws.read_status()

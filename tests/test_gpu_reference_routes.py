@@ -74,7 +74,8 @@ def images():
     return out
 
 
-@pytest.mark.parametrize("tile,warps", [(32, -2), (32, -4), (32, 8), (64, 16)])
+@pytest.mark.parametrize("tile,warps", [(32, -2), (32, -4), (32, 8), (64, -4),
+                                        (64, 16)])
 def test_product_matches_reference_routes(tile, warps):
     pkg = package()
     lib = ref_lib(tile)
