@@ -671,6 +671,7 @@ def summary(line):
         "single_2040x1356": get("single_image_2040x1356", "gpix_s"),
         "launch_floor_us_1_4": [get("launch_floor_2040x1356", "us_1_launch"),
                                 get("launch_floor_2040x1356", "us_4_launch")],
+        "single_passes_us": line.get("single_image_passes_us"),
         "e2e": get("e2e", "value"),
         "tile_pass_frac": get("roofline", "frac"),
     }
@@ -860,6 +861,8 @@ def secondary(args, pkg, plan, images, host_images, maxs, mins, stream, dist,
         out["launch_floor_2040x1356"] = launch_floor_section(
             pkg, images[0].device, stream, len(large), args.warmup,
             args.steps)
+        out["single_image_passes_us"] = single_image_passes(
+            pkg, images[large[0]], stream, args.warmup, 50, tile)
     return out
 
 
@@ -898,6 +901,27 @@ def launch_floor_section(pkg, device, stream, n_images, warmup, reps):
     for k in (1, 4):
         ms = _graph_ms(lambda: run(k), stream, warmup, reps)
         out[f"us_{k}_launch"] = round(ms / n_images * 1e3, 3)
+    return out
+
+
+def single_image_passes(pkg, image, stream, warmup, reps, tile=32):
+    """Device microseconds of each pass of the route on one image (graph of
+    `reps` back-to-back launches of that pass; each pass is idempotent on a
+    workspace where the earlier passes already ran)."""
+    import torch
+    mx = torch.empty_like(image)
+    mn = torch.empty_like(image)
+    plan = pkg.BatchPlan([image], [mx], [mn], tile=tile, stream=stream)
+    ws = plan.make_workspace(stream=stream)
+    plan.run(ws, stream=stream)
+    stream.synchronize()
+    out = {}
+    for name, which in (("tile", 1), ("seam_flags", 4), ("resolve", 2)):
+        def fn(w=which):
+            for _ in range(reps):
+                plan.run_pass(ws, w, stream=stream)
+        out[name] = round(_graph_ms(fn, stream, 1, 1) / reps * 1e3, 3)
+    ws.read_status(stream)
     return out
 
 
@@ -1046,11 +1070,11 @@ def uneven_section(args, pkg, device, stream):
     out["autotuned"] = {
         "gpix_s": round(pixels / ms / 1e6, 3), "ms": round(ms, 4),
         "launches": 1 if tb.single is not None else len(tb.parts),
-        "form": ("one default launch (faster than the tuned choices on "
-                 "this batch)" if tb.single is not None
-                 else "the tuned choices"),
+        "form": tb.form,
+        "forms_ms": tb.timings_ms,
         "tuning_s": round(tune_s, 1),
         "choices": {str(k): v.label() for k, v in table.choices.items()},
+        "mix_choice": table.mix.label() if table.mix else None,
         "class_bounds_px": list(at.CLASS_BOUNDS[:-1]),
     }
     sample = list(range(0, len(images), 64))

@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define SS_ABI_VERSION 1
+#define SS_ABI_VERSION 2
 
 typedef enum ss_status {
     SS_OK = 0,
@@ -281,6 +281,15 @@ typedef struct ss_launch {
                           * 32 for large ones) */
     int32_t passes;      /* passes to enqueue (1 tile, 4 seam, 2 resolve,
                           * enqueued in that order); 0 = all */
+    int32_t flatten;     /* row-scan kernels: flatten schedule of the seam
+                          * fragments' union-find before the verdicts are
+                          * read.  0 = roots found with path halving in the
+                          * flags pass; 1 = also point every fragment at its
+                          * root there; 2 = a separate pass points every
+                          * fragment at its root first (the reference's
+                          * compress_fragment_parents,
+                          * harness/primary/snapshot_sparse_seam_cuda_v1_0.cu
+                          * :583-599), one more launch */
 } ss_launch;
 
 /* ss_extrema_batch with explicit launch choices (NULL = all defaults). */

@@ -89,6 +89,7 @@ class Launch(ctypes.Structure):
         ("persistent", ctypes.c_int32),
         ("group", ctypes.c_int32),
         ("passes", ctypes.c_int32),
+        ("flatten", ctypes.c_int32),
     ]
 
 
@@ -439,12 +440,13 @@ class BatchPlan:
 
     def run_launch(self, workspace: Workspace, warps: int = 0,
                    persistent: bool = False, group: int = 0, passes: int = 0,
-                   stream=None) -> None:
+                   flatten: int = 0, stream=None) -> None:
         """ss_extrema_batch_launch: explicit kernel family (0 = the tile's
-        default), schedule, seam/resolve tiles per warp (0 = automatic) and
-        passes (0 = all)."""
+        default), schedule, seam/resolve tiles per warp (0 = automatic),
+        passes (0 = all) and fragment flatten schedule (0 halving, 1
+        compress in the flags pass, 2 separate compress pass)."""
         launch = Launch(int(warps), 1 if persistent else 0, int(group),
-                        int(passes))
+                        int(passes), int(flatten))
         st = lib().ss_extrema_batch_launch(
             self.host_plan.ctypes.data, self.device_plan.data_ptr(),
             self.plan_bytes, ctypes.byref(launch), workspace.ptr,

@@ -120,7 +120,22 @@ struct Source {
     int64_t total_tiles;
     int32_t group;               // tiles per warp in the row-scan seam and
                                  //   resolve passes (power of two, 1..32)
+    int32_t flatten;             // fragment forest flatten schedule of the
+                                 //   row-scan flags pass (kFlatten*)
 };
+
+// Flatten schedules of the fragment union-find after the seam pass (the
+// row-scan route): the flags pass finds each fragment's root with path
+// halving (kFlattenHalve); or also points the fragment straight at its root
+// (kFlattenCompress), so the resolve pass's finds take one step; or a
+// separate pass first points every fragment at its root, as the
+// reference's compress_fragment_parents does
+// (harness/primary/snapshot_sparse_seam_cuda_v1_0.cu:583-599), and the flags
+// pass then finds roots in one step (kFlattenSeparate; one more launch).
+constexpr int32_t kFlattenHalve = 0;
+constexpr int32_t kFlattenCompress = 1;
+constexpr int32_t kFlattenSeparate = 2;
+constexpr int32_t kFlattenOnly = 3;      // the separate pass itself
 
 // Device view of the workspace arrays (global tile index g, slot s).
 struct Arena {

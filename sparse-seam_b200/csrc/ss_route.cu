@@ -863,7 +863,7 @@ bool workspace_bytes_for_tiles(int64_t tiles, int tile, size_t* bytes) {
 static ss_status launch_route(const Config& cfg, const Source& src_in,
                               const Arena& arena, int persistent,
                               cudaStream_t stream, int passes = 7,
-                              int group = 0) {
+                              int group = 0, int flatten = kFlattenHalve) {
     if (src_in.total_tiles == 0) {
         return SS_OK;
     }
@@ -907,6 +907,13 @@ static ss_status launch_route(const Config& cfg, const Source& src_in,
         cfg.seam_pass<<<static_cast<unsigned>(ctas2), later_threads, 0,
                         stream>>>(src, arena);
         if (cfg.flags_pass) {
+            src.flatten = flatten;
+            if (flatten == kFlattenSeparate) {
+                Source only = src;
+                only.flatten = kFlattenOnly;
+                cfg.flags_pass<<<static_cast<unsigned>(ctas2), later_threads,
+                                 0, stream>>>(only, arena);
+            }
             cfg.flags_pass<<<static_cast<unsigned>(ctas2), later_threads, 0,
                              stream>>>(src, arena);
         }
@@ -1274,12 +1281,15 @@ static ss_status batch_passes(const void* h_plan, const void* d_plan,
                               size_t plan_bytes, int persistent,
                               void* d_workspace, size_t workspace_bytes,
                               void* stream, int passes, int warps = 0,
-                              int group = 0) {
+                              int group = 0, int flatten = kFlattenHalve) {
     if (!h_plan || !d_plan || !d_workspace ||
         plan_bytes < sizeof(PlanHeader)) {
         return SS_ERR_INVALID_VALUE;
     }
     if (group != 0 && (group < 0 || group > 32 || (group & (group - 1)))) {
+        return SS_ERR_INVALID_VALUE;
+    }
+    if (flatten < kFlattenHalve || flatten > kFlattenSeparate) {
         return SS_ERR_INVALID_VALUE;
     }
     if (reinterpret_cast<uintptr_t>(d_workspace) % 256 != 0 ||
@@ -1318,7 +1328,8 @@ static ss_status batch_passes(const void* h_plan, const void* d_plan,
     src.total_tiles = ph->total_tiles;
     return launch_route(*cfg, src, arena_at(d_workspace, L),
                         persistent ? 1 : 0,
-                        static_cast<cudaStream_t>(stream), passes, group);
+                        static_cast<cudaStream_t>(stream), passes, group,
+                        flatten);
 }
 
 ss_status ss_extrema_batch(const void* h_plan, const void* d_plan,
@@ -1342,7 +1353,7 @@ ss_status ss_extrema_batch_launch(const void* h_plan, const void* d_plan,
     }
     return batch_passes(h_plan, d_plan, plan_bytes, l.persistent ? 1 : 0,
                         d_workspace, workspace_bytes, stream,
-                        l.passes ? l.passes : 7, l.warps, l.group);
+                        l.passes ? l.passes : 7, l.warps, l.group, l.flatten);
 }
 
 ss_status ss_extrema_batch_pass(const void* h_plan, const void* d_plan,

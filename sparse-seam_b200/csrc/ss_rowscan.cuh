@@ -267,9 +267,16 @@ __device__ __forceinline__ void flags_pass_group(const Source& src,
             const int fr = static_cast<int>((first + owner) * kSlots + r);
             const int root = global_find(a.parent, fr, err);
             if (root != fr) {
-                const uint32_t own = ld_relaxed(a.bits + fr) & 3u;
-                if (own && (ld_relaxed(a.bits + root) & own) != own) {
-                    atomicOr(a.bits + root, own);
+                // Pointing a fragment at its root is safe at any time after
+                // the links: every reader sees an ancestor either way.
+                if (src.flatten != kFlattenHalve) {
+                    st_relaxed(a.parent + fr, root);
+                }
+                if (src.flatten != kFlattenOnly) {
+                    const uint32_t own = ld_relaxed(a.bits + fr) & 3u;
+                    if (own && (ld_relaxed(a.bits + root) & own) != own) {
+                        atomicOr(a.bits + root, own);
+                    }
                 }
             }
         }

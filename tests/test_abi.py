@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
 def test_status_strings_and_version():
     pkg = package()
     lib = pkg.lib()
-    assert lib.ss_abi_version() == 1
+    assert lib.ss_abi_version() == 2
     for code, name in pkg.STATUS.items():
         assert lib.ss_status_string(code).decode() == name
     assert lib.ss_status_string(999).decode() == "SS_ERR_UNKNOWN"

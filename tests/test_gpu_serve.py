@@ -154,25 +154,40 @@ def test_autotuned_batch_matches_oracle():
     at = importlib.import_module("sparse-seam_b200.autotune")
     synth = importlib.import_module("sparse-seam_b200.synth")
     choices = [c for c in at.candidates()
-               if (c.tile == 32 and c.group in (0, 1)) or
+               if (c.tile == 32 and c.group in (0, 4)) or
                (c.tile in (16, 64) and not c.persistent)]
+    assert {c.flatten for c in choices} == {0, 1, 2}
     table = at.tune(pixels_per_class=1 << 19, reps=1, classes=(0, 1, 2, 3),
-                    choices=choices)
+                    choices=choices, mix_images=24)
     assert set(table.choices) == {0, 1, 2, 3}
+    assert table.mix in choices
     images = synth.uneven_batch(40, seed=21, lo=16, hi=900, device="cuda")
     maxs = [torch.empty_like(i) for i in images]
     mins = [torch.empty_like(i) for i in images]
     tb = at.TunedBatch(images, maxs, mins, table)
     wants = [oracle.extrema(im.cpu().numpy()) for im in images]
-    # The form `run` picked, then the split by size class itself.
+    assert tb.form in tb.timings_ms
+    mix = table.mix
+    whole = pkg_plan = None
+    import importlib as _il
+    pkg = _il.import_module("sparse-seam_b200")
+    pkg_plan = pkg.BatchPlan(images, maxs, mins, tile=mix.tile)
+    whole = pkg_plan.make_workspace()
+    # The form `run` picked, the split by size class itself, and one launch
+    # with the mix's choice.
     for form in (tb.run,
-                 lambda: tb._run_parts(torch.cuda.current_stream())):
+                 lambda: tb._run_parts(torch.cuda.current_stream()),
+                 lambda: pkg_plan.run_launch(whole, warps=mix.warps,
+                                             persistent=mix.persistent,
+                                             group=mix.group,
+                                             flatten=mix.flatten)):
         for m in maxs + mins:
             m.fill_(5)
         form()
         torch.cuda.synchronize()
         for part in tb.parts:
             part[2].read_status()
+        whole.read_status()
         for i, want in enumerate(wants):
             assert np.array_equal(maxs[i].cpu().numpy(), want[0]), i
             assert np.array_equal(mins[i].cpu().numpy(), want[1]), i

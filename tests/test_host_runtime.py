@@ -69,6 +69,10 @@ def test_batch_launch_rejects_bad_choices():
     assert lib.ss_extrema_batch_launch(fake, fake, 4096,
                                        ctypes.byref(bad_passes), fake, 4096,
                                        None) == 1
+    bad_flatten = pkg.Launch(0, 0, 0, 0, 3)
+    assert lib.ss_extrema_batch_launch(fake, fake, 4096,
+                                       ctypes.byref(bad_flatten), fake, 4096,
+                                       None) == 1
     assert lib.ss_extrema_batch_launch(None, fake, 4096, None, fake, 4096,
                                        None) == 1
 
@@ -89,10 +93,12 @@ def test_autotuner_tables():
     for tile, family in pkg.KERNEL_CONFIGS.items():
         for w in family:
             assert any(c.tile == tile and c.warps == w for c in cands)
+    assert {c.flatten for c in cands if c.warps < 0} == {0, 1, 2}
     table = at.TuningTable({k: cands[k] for k in range(4)},
-                           {0: {"x": 1.0}})
+                           {0: {"x": 1.0}}, cands[5], {"y": 2.0})
     back = at.TuningTable.from_json(table.to_json())
     assert back.choices == table.choices
+    assert back.mix == cands[5] and back.mix_timings_ms == {"y": 2.0}
     assert back.choice_for(700, 700) == cands[3]
 
 
