@@ -72,6 +72,9 @@ def parse_args():
                         "sections")
     p.add_argument("--passes-only", action="store_true",
                    help="only run the split-pass loop (for profiling)")
+    p.add_argument("--host-only", action="store_true",
+                   help="only run the host-to-host form (pack kernel and "
+                        "host expansion; for profiling)")
     p.add_argument("--levels", type=int, default=256,
                    help="re-quantise the corpus to this many gray levels")
     p.add_argument("--sweep", action="store_true",
@@ -513,6 +516,15 @@ def main():
             plan.run_pass(ws, 4, stream=stream)
             plan.run_pass(ws, 2, stream=stream)
         ws.read_status(stream)
+        return 0
+    if args.host_only:
+        host = import_module("sparse-seam_b200.host")
+        hb = host.HostBatch(host_images, tile=tile, chunks=16,
+                            persistent=False, packed=True)
+        for _ in range(max(1, args.steps)):
+            hb.run(stream)
+        stream.synchronize()
+        hb.check()
         return 0
 
     # -- schedule: one CTA per work item vs the persistent work queue -------
