@@ -842,19 +842,28 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
     hm_rows[y] = 0u;
     hn_rows[y] = 0u;
     lv_rows[y] = 0u;
-    uint32_t n_list = 0;
-    const uint32_t list_at = warp_prefix(__popc(loop_heads), n_list);
+    // The undecided runs come first in the list (the verdict loop visits
+    // only them), the others after: one prefix over both counts (16 bits
+    // each; a tile has at most 1,024 runs).
+    uint32_t both = 0;
+    const uint32_t at = warp_prefix(
+        __popc(loop_heads & undecided) | (__popc(loop_heads & ~undecided) << 16),
+        both);
+    const uint32_t n_und = both & 0xFFFFu;
+    const uint32_t n_list = n_und + (both >> 16);
     const bool listed = n_list <= static_cast<uint32_t>(kListCap);
     if (listed) {
         uint32_t r = loop_heads;
-        uint32_t k = list_at;
+        uint32_t ku = at & 0xFFFFu;
+        uint32_t ko = n_und + (at >> 16);
         while (r) {
             const int h = __ffs(r) - 1;
             r &= r - 1u;
-            list[k++] = static_cast<uint16_t>(
+            const uint32_t und = (undecided >> h) & 1u;
+            list[und ? ku++ : ko++] = static_cast<uint16_t>(
                 y | (h << 5) | (((own_gt >> h) & 1u) << 10) |
                 (((own_lt >> h) & 1u) << 11) | (((own_seam >> h) & 1u) << 12) |
-                (((undecided >> h) & 1u) << 13));
+                (und << 13));
         }
     }
     // Steps of the two loops: 32 runs each, or the busiest row's runs.
@@ -862,17 +871,17 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
         listed ? static_cast<int>((n_list + 31u) >> 5)
                : static_cast<int>(__reduce_max_sync(~0u, __popc(loop_heads)));
     const int steps_und =
-        listed ? steps_all
+        listed ? static_cast<int>((n_und + 31u) >> 5)
                : static_cast<int>(
                      __reduce_max_sync(~0u, __popc(loop_heads & undecided)));
     __syncwarp();
     // The run a lane takes at step `it`: from the list, or the next of its
     // row's runs in `r` (row order).  Returns false when it has none.
-    auto take = [&](int it, uint32_t& r, int& yy, int& h, uint32_t& own,
-                    bool& und) -> bool {
+    auto take = [&](int it, uint32_t lim, uint32_t& r, int& yy, int& h,
+                    uint32_t& own, bool& und) -> bool {
         if (listed) {
             const uint32_t idx = static_cast<uint32_t>(it * 32 + lane);
-            if (idx >= n_list) {
+            if (idx >= lim) {
                 return false;
             }
             const uint32_t e = list[idx];
@@ -903,7 +912,7 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
             int yy = 0, h = 0;
             uint32_t own = 0u;
             bool und = false;
-            if (take(it, r, yy, h, own, und)) {
+            if (take(it, n_list, r, yy, h, own, und)) {
                 const int p = wb + run_word(yy, h);
                 // The walk keeps the root's word: the flags read from it may
                 // lag other lanes' ORs, which only costs a redundant OR.
@@ -958,7 +967,7 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
             uint32_t rec1 = 0u;
             uint32_t own = 0u;
             bool und = false;
-            if (take(it, r, yy, h, own, und) && und) {
+            if (take(it, n_und, r, yy, h, own, und) && und) {
                 const int p = wb + run_word(yy, h);
                 root = rparent(vw[p], p);
                 const uint32_t w = vw[root];
@@ -1043,7 +1052,7 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
                 uint32_t own = 0u, w = 0u;
                 bool und = false;
                 bool live_root = false;
-                if (take(it, r, yy, h, own, und)) {
+                if (take(it, n_list, r, yy, h, own, und)) {
                     p = wb + run_word(yy, h);
                     w = vw[p];
                     const uint32_t z = (w >> kZoneShift) & 7u;
@@ -1081,7 +1090,7 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
             uint32_t rec1 = 0u;
             uint32_t own = 0u;
             bool und = false;
-            if (take(it, r, yy, h, own, und) && und) {
+            if (take(it, n_und, r, yy, h, own, und) && und) {
                 p = wb + run_word(yy, h);
                 root = rparent(vw[p], p);
                 const uint32_t w = vw[root];
