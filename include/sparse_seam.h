@@ -149,8 +149,8 @@ ss_status ss_empty_launches(int count, int grid, int threads, void* stream);
  * the library; this call allocates nothing (no cudaMalloc, no allocating
  * library routine).
  * Limits: images whose ss_workspace_bytes exceeds 32 MiB are rejected with
- * SS_ERR_EXCEEDS_STATIC_SCRATCH (at T = 32 about 4.6 Mpixel, e.g. 2040 x 1356;
- * at T = 64 about 50 Mpixel).
+ * SS_ERR_EXCEEDS_STATIC_SCRATCH (at T = 32 about 4.8 Mpixel, e.g. 2040 x 1356
+ * or 2208 x 2208; at T = 64 about 5.9 Mpixel; at T = 16 about 14 Mpixel).
  * Set-up: the array lives in its own module, which the driver loads (and so
  * allocates the 32 MiB) the first time this call or
  * ss_static_scratch_read_status runs in a CUDA context; the first call in a
