@@ -437,9 +437,6 @@ __global__ void empty_kernel() {}
 // Row-scan kernels (T = 32): NW independent warps per CTA, one tile each.
 // ---------------------------------------------------------------------------
 
-// Most items a warp of the persistent row-scan tile pass takes per pop.
-constexpr uint32_t kQueueChunk = 16u;
-
 // Row-scan tile pass: NW independent warps per CTA, one tile each; at most
 // 64 registers per thread, so 32 warps fit on an SM (the shared-memory
 // limit at 6.4 KB per warp).  The persistent form's work loop holds a few
@@ -462,35 +459,22 @@ runs_tile_pass_kernel(Source src, Arena a) {
         a.header->route = 1u;
     }
     if constexpr (kPersistent) {
-        // Guided self-scheduling: each pop takes a run of consecutive items
-        // sized to the work left (half of an even share per warp, at most
-        // kQueueChunk), so most items cost no atomic on the shared cursor
-        // and the last ones go out singly, keeping the tail short.
-        const int64_t warps = static_cast<int64_t>(gridDim.x) * NW;
+        // One item per pop: the tiles in flight stay a window of consecutive
+        // items, like the grid schedule's, so neighbouring tiles' halo rows
+        // and mask sectors meet in L2 (runs of 4 or 16 items per pop spread
+        // the window over tens of thousands of tiles and measured slower).
         for (;;) {
-            uint32_t first = 0;
-            uint32_t count = 1;
+            uint32_t item = 0;
             if (lane == 0) {
-                const int64_t left =
-                    src.total_tiles - static_cast<int64_t>(ld_relaxed(
-                                          &a.header->queue_head));
-                count = static_cast<uint32_t>(
-                    max(int64_t(1), min(static_cast<int64_t>(kQueueChunk),
-                                        left / (2 * warps))));
-                first = atomicAdd(&a.header->queue_head, count);
+                item = atomicAdd(&a.header->queue_head, 1u);
             }
-            first = __shfl_sync(~0u, first, 0);
-            count = __shfl_sync(~0u, count, 0);
-            if (static_cast<int64_t>(first) >= src.total_tiles) {
+            item = __shfl_sync(~0u, item, 0);
+            if (static_cast<int64_t>(item) >= src.total_tiles) {
                 break;
             }
-            const int64_t end = min(src.total_tiles,
-                                    static_cast<int64_t>(first) + count);
-            for (int64_t item = first; item < end; ++item) {
-                rowscan::tile_pass_runs<1>(sm[warp].word, sm[warp].aux,
-                                           nullptr, 0, src, a, item);
-                __syncwarp();
-            }
+            rowscan::tile_pass_runs<1>(sm[warp].word, sm[warp].aux, nullptr,
+                                       0, src, a, item);
+            __syncwarp();
         }
     } else {
         const int64_t item = static_cast<int64_t>(blockIdx.x) * NW + warp;
