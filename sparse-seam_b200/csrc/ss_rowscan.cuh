@@ -472,7 +472,9 @@ __device__ __forceinline__ void resolve_group(ResolveSmem<TT>& sm,
                           ((fl & kHasSmaller) ? 0u : 0xFF00u);
                 off = sm.out_origin[owner] +
                       static_cast<int64_t>(y) * sm.out_pitch[owner] + x;
-                len = static_cast<uint32_t>(n_px);
+                // A zone in neither mask keeps the tile pass's placeholder
+                // bytes (0, 0): nothing to write.
+                len = verdict ? static_cast<uint32_t>(n_px) : 0u;
             }
         }
         uint32_t bytes = 0u;
@@ -525,6 +527,9 @@ __device__ __forceinline__ void resolve_group(ResolveSmem<TT>& sm,
                 continue;
             }
             const uint32_t fl = sm.final_flags[t][rec];
+            if ((fl & kDead) == kDead) {
+                continue;   // in neither mask: the placeholder bytes stand
+            }
             const Row R = ((Row(2) << (x + n_px - 1)) - Row(1)) &
                           ~((Row(1) << x) - Row(1));
             atomicOr(&live_rows[y], R);

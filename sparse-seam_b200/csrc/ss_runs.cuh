@@ -1141,9 +1141,10 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
     // The tile's logged pixels (a statistic: bits 16-31 of its log count).
     const uint32_t logged_px = __reduce_add_sync(~0u, live_px);
     // The mask bytes of every pixel of the tile.  Pixels of live zones get a
-    // placeholder 0 here and their final bytes from the resolve pass, which
-    // runs after this pass; so whole rows are written, with 16-, 8- or
-    // 4-byte stores where the output rows allow it.
+    // placeholder 0 in both masks here; the resolve pass, which runs after
+    // this pass, rewrites those of zones that end up in a mask (most end up
+    // in neither, and their placeholders are final).  So whole rows are
+    // written, with 16-, 8- or 4-byte stores where the output rows allow it.
     {
         const uint64_t bmx = reinterpret_cast<uint64_t>(
             omax + static_cast<int64_t>(g.y0) * out_pitch + g.x0);
