@@ -127,9 +127,10 @@ typedef struct ss_stats {
  * process (the autotuner's hook; the masks never depend on it).
  *   warps > 0   CTA-per-tile kernels with `warps` warps per CTA
  *               (tile 16: 2, 4 or 8; tile 32: 4, 8 or 16; tile 64: 8 or 16)
- *   warps < 0   tile 32 only: row-scan kernels (per-row bit masks and runs),
- *               one tile per warp, -warps warps per CTA (2 or 4)
- * Defaults: tile 16 -> 4, tile 32 -> -2, tile 64 -> 16.  The reference fixes
+ *   warps < 0   row-scan kernels (per-row bit masks and runs): tile 32, one
+ *               tile per warp, -warps warps per CTA (2 or 4); tile 64 (-4),
+ *               one tile per CTA of four warps, one per 32 x 32 quadrant
+ * Defaults: tile 16 -> 4, tile 32 -> -2, tile 64 -> -4.  The reference fixes
  * its tile and classify threads at compile time
  * (harness/configuration_study/sparse_config_benchmark_v0_8.cu:17-30). */
 ss_status ss_set_kernel_config(int tile, int warps);

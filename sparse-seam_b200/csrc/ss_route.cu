@@ -1,6 +1,10 @@
 // ss_route.cu -- kernels and C ABI of the exact dual regional-extrema route.
 //
-// Two kernels per call, for one image or a whole batch:
+// Two kernel families.  The row-scan family (the default at tile edges 32
+// and 64; ss_runs.cuh, ss_rowscan.cuh) runs a tile pass, a seam pass, a
+// flags pass and a resolve pass.  The CTA-per-tile family (the default at
+// tile edge 16, selectable at every edge), defined below, runs two kernels
+// per call, for one image or a whole batch:
 //
 //   tile pass    per (image, tile): label the tile, write both masks (final
 //                for zones inside the tile, provisional -- from the tile's own
@@ -434,7 +438,8 @@ __global__ void init_header_kernel(Header* h) {
 __global__ void empty_kernel() {}
 
 // ---------------------------------------------------------------------------
-// Row-scan kernels (T = 32): NW independent warps per CTA, one tile each.
+// Row-scan kernels: tile pass (T = 32: NW independent warps per CTA, one tile
+// each; T = 64: four quadrant warps per tile), seam, flags, resolve passes.
 // ---------------------------------------------------------------------------
 
 // Row-scan tile pass: NW independent warps per CTA, one tile each; at most

@@ -1,6 +1,7 @@
-// ss_rowscan.cuh -- the T = 32 route (the reference's reported tile size):
-// shared definitions and the passes after the tile pass.  The tile pass
-// itself (one warp per tile, per-row bit masks and runs) is ss_runs.cuh.
+// ss_rowscan.cuh -- the row-scan route (tile edge 32, the reference's
+// reported setting, and 64): shared definitions and the passes after the
+// tile pass, templated on the tile edge.  The tile pass itself (per-row bit
+// masks and runs; one warp per 32 x 32 tile or quadrant) is ss_runs.cuh.
 //
 // Observation the design rests on: a pixel with both a strictly greater and a
 // strictly smaller 8-neighbour ("decided" pixel) is in neither mask, and
