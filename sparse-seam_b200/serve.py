@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes
 import importlib
+import os
 import time
 from dataclasses import dataclass
 from typing import Callable, Dict, List, Optional, Sequence, Tuple
@@ -73,6 +74,29 @@ class Server:
         self._keep[int(ticket.value)] = (image, maxima, minima)
         return int(ticket.value)
 
+    def submit_file(self, path: str, user: int = 0):
+        """Decodes an image file (PGM, PNG, BMP, JPEG or TIFF, read as the
+        reference's cv::imread(path, IMREAD_GRAYSCALE) reads it) straight
+        into pinned host memory and queues it.  Returns (ticket, maxima,
+        minima): the masks arrive in the returned pinned buffers when the
+        request's completion is polled."""
+        import torch
+        w, h = ctypes.c_int(0), ctypes.c_int(0)
+        p = os.fsencode(path)
+        _pkg._check(_pkg.lib().ss_read_image(p, None, 0, ctypes.byref(w),
+                                             ctypes.byref(h)),
+                    f"ss_read_image({path})")
+        shape = (h.value, w.value)
+        pin = dict(dtype=torch.uint8, pin_memory=True)
+        image = torch.empty(shape, **pin)
+        _pkg._check(_pkg.lib().ss_read_image(p, image.data_ptr(),
+                                             image.numel(), ctypes.byref(w),
+                                             ctypes.byref(h)),
+                    f"ss_read_image({path})")
+        maxima = torch.empty(shape, **pin)
+        minima = torch.empty(shape, **pin)
+        return self.submit(image, maxima, minima, user=user), maxima, minima
+
     def poll(self, timeout_us: int = 0) -> List[Completion]:
         n = ctypes.c_int(0)
         _pkg._check(_pkg.lib().ss_server_poll(self._h, self._buf,
@@ -114,6 +138,30 @@ class Server:
 # ---------------------------------------------------------------------------
 # Open-loop load
 # ---------------------------------------------------------------------------
+
+def serve_files(server: Server, paths: Sequence[str],
+                timeout_s: float = 600.0) -> Dict[str, Tuple]:
+    """Serves image files: each is decoded into pinned memory and queued as
+    soon as it is read (decoding the next file overlaps the GPU work of the
+    earlier ones).  Returns {path: (maxima, minima)}; raises on a failed
+    request."""
+    pending = {}
+    for i, path in enumerate(paths):
+        ticket, mx, mn = server.submit_file(path, user=i)
+        pending[ticket] = (path, mx, mn)
+    out = {}
+    deadline = time.monotonic() + timeout_s
+    while len(out) < len(paths):
+        if time.monotonic() > deadline:
+            raise TimeoutError("requests did not complete in time")
+        for c in server.poll(timeout_us=10_000):
+            path, mx, mn = pending[int(c.ticket)]
+            if c.status != 0:
+                raise _pkg.SparseSeamError(int(c.status),
+                                           f"served request {path}")
+            out[path] = (mx, mn)
+    return out
+
 
 def poisson_trace(rate: float, duration_s: float, seed: int = 0) -> np.ndarray:
     """Arrival offsets in nanoseconds of a Poisson process."""

@@ -240,3 +240,33 @@ def test_large_requests_come_back_compact():
         want = oracle.extrema(im.numpy(), method="bands", threads=8)
         assert np.array_equal(outs[i][0].numpy(), want[0]), i
         assert np.array_equal(outs[i][1].numpy(), want[1]), i
+
+
+def test_served_files_match_oracle(tmp_path):
+    """Image files decoded by the library straight into pinned buffers and
+    served: every result equals the oracle's on the decoded pixels."""
+    serve = importlib.import_module("sparse-seam_b200.serve")
+    synth = importlib.import_module("sparse-seam_b200.synth")
+    pkg = package()
+    rng = np.random.default_rng(31)
+    paths = []
+    for i, (h, w) in enumerate([(321, 481), (700, 1029), (64, 64),
+                                (1356, 2040)]):
+        img = synth.quantize(synth.smooth_noise_np(h, w, 40 + i),
+                             int(rng.integers(2, 257)))
+        p = tmp_path / f"img_{i}.pgm"
+        pkg.write_pgm(str(p), img)
+        paths.append(str(p))
+    cv2 = pytest.importorskip("cv2")
+    img = synth.smooth_noise_np(500, 333, 77)
+    p = tmp_path / "img_png.png"
+    assert cv2.imwrite(str(p), img)
+    paths.append(str(p))
+    with serve.Server(tile=32, inflight=2, max_batch_images=8,
+                      batch_tiles=1 << 14, pool_bytes=64 << 20) as srv:
+        out = serve.serve_files(srv, paths)
+    for path in paths:
+        want = oracle.extrema(pkg.read_image(path))
+        mx, mn = out[path]
+        assert np.array_equal(mx.numpy(), want[0]), path
+        assert np.array_equal(mn.numpy(), want[1]), path
