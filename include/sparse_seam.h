@@ -310,7 +310,10 @@ ss_status ss_extrema_batch_launch(const void* h_plan, const void* d_plan,
  * masks with `threads` host threads (0 = all processors but one), and
  * ss_enqueue_unpack_masks
  * does the same as a host function enqueued on `stream` (ordered after the
- * stream's earlier work; the buffers must stay valid until it runs).  No
+ * stream's earlier work; the buffers must stay valid until it runs; 0 = a
+ * quarter of the processors, at least one: the expansion then overlaps
+ * host-to-device copies that read the same host memory, and more threads
+ * slow those copies more than they speed the expansion).  No
  * counterpart in the reference, which copies both byte masks back
  * (harness/primary/gpu_common_v0_6.cu:351-373). */
 ss_status ss_pack_masks(const uint8_t* d_maxima, const uint8_t* d_minima,
