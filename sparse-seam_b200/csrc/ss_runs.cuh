@@ -1,11 +1,12 @@
 // ss_runs.cuh -- the T = 32 tile pass: one warp per 32 x 32 tile, on
 // per-row bit masks and runs.
 //
-// The tile and its one-pixel halo are staged in shared memory (int16, -1
-// outside the image).  A row scan (lane = column) finds each pixel's
-// greater / smaller flags from sliding 3 x 3 maxima / minima (a signed max
-// and an unsigned min both ignore -1); "decided" pixels have both and are in
-// neither mask, with their whole zone.  The scan leaves seven 32-bit masks
+// The tile and its one-pixel halo are staged in shared memory, rows t and
+// t + 16 paired in one word as two half-precision numbers (NaN outside the
+// image).  A row scan (lane = column, two rows per step) finds each pixel's
+// greater / smaller flags from sliding 3 x 3 pair maxima / minima (both pass
+// over NaN); "decided" pixels have both and are in neither mask, with their
+// whole zone.  The scan leaves seven 32-bit masks
 // per tile row in the registers of lane y = row:
 //   L    listed pixels (not decided)
 //   GT   listed pixels with a strictly greater 8-neighbour
@@ -50,14 +51,66 @@ namespace ss {
 
 namespace rowscan {
 
+// The staged square pairs row r with row r + 16 in one 32-bit word: slot s
+// (0 .. 17) of staged column c holds staged row s in its low half and staged
+// row s + 16 in its high half, so one row-scan step handles tile rows t and
+// t + 16 with half-precision pair max / min.  A pixel value v is staged as
+// the half 1024 + v (bits 0x6400 | v: exact, ordered, equal iff the values
+// are), a pixel outside the image as 0xFFFF, a NaN, which max and min pass
+// over.  Staged rows 16 and 17 sit in both halves (low of slots 16, 17;
+// high of 0, 1).
+constexpr int kSlotRows = T / 2 + 2;
+constexpr uint32_t kStageBias = 0x6400u;   // half-precision 1024
+
+__device__ __forceinline__ int16_t stage_code(int v) {
+    return static_cast<int16_t>(v >= 0 ? static_cast<int>(kStageBias) | v
+                                       : -1);
+}
+
 // Per warp (one 32 x 32 square): the seam equality masks kept for the end
-// of the pass, and the staged square (its image pixels + halo, -1 outside
-// the image; staged pixel (c, r) at index 1 + r * kHaloW + c, so that
-// columns 4k, 4k + 1 share a word), later reused for the run list.
+// of the pass, and the staged square (its image pixels + halo; slot s of
+// staged column c at word 1 + s * kHaloW + c, so that tile columns 4k and
+// 4k + 1 share an 8-byte boundary), later reused for the run list.
 struct __align__(16) RunAux {
     uint32_t eq[16];
-    int16_t img[kHaloW * kHaloW + 2];
+    uint32_t img[kSlotRows * kHaloW + 2];
 };
+static_assert(sizeof(uint32_t) * (kSlotRows * kHaloW + 2) >=
+                  sizeof(uint16_t) * kListCap + sizeof(uint32_t) * 3 * T,
+              "the run list and its row masks reuse the staged square");
+
+// Pair maximum / minimum of two staged words, both halves at once; a NaN
+// half (outside the image) yields the other operand's half, and a number
+// comes back bit for bit.
+__device__ __forceinline__ uint32_t max_pair(uint32_t a, uint32_t b) {
+    uint32_t d;
+    asm("max.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+__device__ __forceinline__ uint32_t min_pair(uint32_t a, uint32_t b) {
+    uint32_t d;
+    asm("min.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+
+// Warp ballots of a pair comparison: bit `lane` of lo / hi is the comparison
+// of the lanes' low / high halves (one compare for both, false where either
+// half is a NaN).  Every lane of the warp must call it.
+#define SS_PAIR_BALLOT(NAME, CMP)                                            \
+    __device__ __forceinline__ void NAME(uint32_t a, uint32_t b,            \
+                                         uint32_t& lo, uint32_t& hi) {      \
+        asm volatile(                                                       \
+            "{\n\t.reg .pred p, q;\n\t"                                     \
+            "setp." CMP ".f16x2 p|q, %2, %3;\n\t"                           \
+            "vote.sync.ballot.b32 %0, p, 0xffffffff;\n\t"                   \
+            "vote.sync.ballot.b32 %1, q, 0xffffffff;\n\t}"                  \
+            : "=r"(lo), "=r"(hi)                                            \
+            : "r"(a), "r"(b));                                              \
+    }
+SS_PAIR_BALLOT(ballot_pair_gt, "gt")
+SS_PAIR_BALLOT(ballot_pair_lt, "lt")
+SS_PAIR_BALLOT(ballot_pair_eq, "eq")
+#undef SS_PAIR_BALLOT
 
 // Tile edge 32: one warp per tile, its own words.
 struct __align__(16) RunSmem {
@@ -300,11 +353,13 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
     const int64_t out_pitch = job.out_pitch;
     uint8_t* __restrict__ omax = job.maxima;
     uint8_t* __restrict__ omin = job.minima;
-    int16_t* const simg = ax.img + 1;
+    uint32_t* const simg = ax.img + 1;
+    int16_t* const shalf = reinterpret_cast<int16_t*>(simg);
 
     // -- prologue: stage the tile and its halo; zero the words --------------
     // Staged row r holds image row y0 - 1 + r, staged column c image column
-    // x0 - 1 + c.
+    // x0 - 1 + c; slot s of column c (word s * kHaloW + c of simg) pairs
+    // staged rows s and s + 16.
     {
         // Optional re-quantisation of every loaded pixel through a 256-entry
         // table in the (not yet used) union-find words, built before the
@@ -346,21 +401,30 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
                       ? static_cast<int>(__ldg(img + gy1 * pitch + xr))
                       : -1;
         };
+        // Staged row r, column c, into its half-word(s).
+        auto put = [&](int r, int c, int16_t v) {
+            if (r < kSlotRows) {
+                shalf[2 * (r * kHaloW + c)] = v;
+            }
+            if (r >= T / 2) {
+                shalf[2 * ((r - T / 2) * kHaloW + c) + 1] = v;
+            }
+        };
         auto store_halo = [&](int16_t hl0, int16_t hr0, int16_t hl1,
                               int16_t hr1) {
-            simg[lane * kHaloW] = hl0;
-            simg[lane * kHaloW + kHaloW - 1] = hr0;
+            put(lane, 0, hl0);
+            put(lane, kHaloW - 1, hr0);
             if (lane < 2) {
-                simg[(32 + lane) * kHaloW] = hl1;
-                simg[(32 + lane) * kHaloW + kHaloW - 1] = hr1;
+                put(32 + lane, 0, hl1);
+                put(32 + lane, kHaloW - 1, hr1);
             }
         };
         int hl0, hr0, hl1, hr1;
         // A tile whose halo lies inside the image, in an image whose rows
         // start on 4-byte boundaries, is read 4 pixels per lane: 8 lanes per
-        // row, 4 rows per load instruction, each word widened to two int16
-        // pairs (tile columns 4k, 4k + 1 sit on a 4-byte boundary of the
-        // staged rows).
+        // row, 4 rows per load instruction.  Lane (k, rr) holds staged rows
+        // rr + 4i, so rows s and s + 16 of its slots s = rr + 4j are its
+        // words j and j + 4, which widen into the slot's 4 packed words.
         const bool word_rows =
             g.tw > 0 && g.th > 0 &&
             !quantise && g.x0 > 0 && g.y0 > 0 && g.x0 + T < width &&
@@ -372,8 +436,7 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
             const int rr = lane >> 3;
             const uint8_t* src =
                 img + static_cast<int64_t>(g.y0 - 1 + rr) * pitch + g.x0 + 4 * k;
-            uint32_t* dst =
-                reinterpret_cast<uint32_t*>(simg + rr * kHaloW + 1 + 4 * k);
+            uint2* dst = reinterpret_cast<uint2*>(simg + rr * kHaloW + 1 + 4 * k);
             uint32_t w[9];
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
@@ -384,14 +447,23 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
             }
             load_halo(hl0, hr0, hl1, hr1);
 #pragma unroll
-            for (int i = 0; i < 9; ++i) {
-                if (i < 8 || rr < 2) {
-                    dst[i * 2 * kHaloW] = __byte_perm(w[i], 0u, 0x4140);
-                    dst[i * 2 * kHaloW + 1] = __byte_perm(w[i], 0u, 0x4342);
+            for (int j = 0; j < 5; ++j) {
+                if (j < 4 || rr < 2) {
+                    // Bytes m of the rows s and s + 16 -> (row s) | (row
+                    // s + 16) << 16 for the slot's columns 4k + m.
+                    const uint32_t t01 = __byte_perm(w[j], w[j + 4], 0x5140);
+                    const uint32_t t23 = __byte_perm(w[j], w[j + 4], 0x7362);
+                    uint2* d = dst + j * 2 * kHaloW;
+                    // Byte 4 of the selector is the bias's high byte.
+                    const uint32_t hb = kStageBias >> 8;
+                    d[0] = make_uint2(__byte_perm(t01, hb, 0x4140),
+                                      __byte_perm(t01, hb, 0x4342));
+                    d[1] = make_uint2(__byte_perm(t23, hb, 0x4140),
+                                      __byte_perm(t23, hb, 0x4342));
                 }
             }
-            store_halo(static_cast<int16_t>(hl0), static_cast<int16_t>(hr0),
-                       static_cast<int16_t>(hl1), static_cast<int16_t>(hr1));
+            store_halo(stage_code(hl0), stage_code(hr0), stage_code(hl1),
+                       stage_code(hr1));
         } else {
             const int gx = g.x0 + lane;
             const bool col_ok = lane < g.tw;
@@ -407,22 +479,26 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
             load_halo(hl0, hr0, hl1, hr1);
             if (quantise) {
                 auto q = [&](int v) -> int16_t {
-                    return static_cast<int16_t>(v >= 0 ? lut[v] : v);
+                    return stage_code(v >= 0 ? lut[v] : v);
                 };
 #pragma unroll
-                for (int r = 0; r < T + 2; ++r) {
-                    simg[r * kHaloW + lane + 1] = q(vals[r]);
+                for (int r = 0; r < kSlotRows; ++r) {
+                    simg[r * kHaloW + lane + 1] =
+                        static_cast<uint16_t>(q(vals[r])) |
+                        static_cast<uint32_t>(
+                            static_cast<uint16_t>(q(vals[r + T / 2]))) << 16;
                 }
                 store_halo(q(hl0), q(hr0), q(hl1), q(hr1));
             } else {
 #pragma unroll
-                for (int r = 0; r < T + 2; ++r) {
-                    simg[r * kHaloW + lane + 1] = static_cast<int16_t>(vals[r]);
+                for (int r = 0; r < kSlotRows; ++r) {
+                    simg[r * kHaloW + lane + 1] =
+                        static_cast<uint16_t>(stage_code(vals[r])) |
+                        static_cast<uint32_t>(static_cast<uint16_t>(
+                            stage_code(vals[r + T / 2]))) << 16;
                 }
-                store_halo(static_cast<int16_t>(hl0),
-                           static_cast<int16_t>(hr0),
-                           static_cast<int16_t>(hl1),
-                           static_cast<int16_t>(hr1));
+                store_halo(stage_code(hl0), stage_code(hr0), stage_code(hl1),
+                           stage_code(hr1));
             }
         }
         __syncwarp();
@@ -443,50 +519,56 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
     // (x, T - 1) equal to pixel (x + d, T) below the tile (d = -1, 0, 1).
     uint32_t bEq[3] = {0u, 0u, 0u};
     {
-        const int16_t* scol = simg + lane;   // staged columns lane .. lane + 2
-        int Lp = scol[0];
-        int vp = scol[1];
-        int Rp = scol[2];
-        int Lc = scol[kHaloW];
-        int vc = scol[kHaloW + 1];
-        int Rc = scol[kHaloW + 2];
-        int hmax_p = max(max(Lp, vp), Rp);
-        unsigned hmin_p = min(min(static_cast<unsigned>(Lp),
-                                  static_cast<unsigned>(vp)),
-                              static_cast<unsigned>(Rp));
-        int hmax_c = max(max(Lc, vc), Rc);
-        unsigned hmin_c = min(min(static_cast<unsigned>(Lc),
-                                  static_cast<unsigned>(vc)),
-                              static_cast<unsigned>(Rc));
-#pragma unroll 8
-        for (int y = 0; y < g.th; ++y) {
-            const int16_t* nrow = scol + (y + 2) * kHaloW;
-            const int Ln = nrow[0];
-            const int vn = nrow[1];
-            const int Rn = nrow[2];
-            const int hmax_n = max(max(Ln, vn), Rn);
-            const unsigned hmin_n =
-                min(min(static_cast<unsigned>(Ln), static_cast<unsigned>(vn)),
-                    static_cast<unsigned>(Rn));
+        // Step t handles tile rows t (low halves) and t + 16 (high halves):
+        // slots t, t + 1, t + 2 hold staged rows t .. t + 2 and t + 16 ..
+        // t + 18.  Rows at or beyond the tile's height give masks that the
+        // pick-up below ignores.
+        const uint32_t* scol = simg + lane;   // staged columns lane .. lane + 2
+        uint32_t Lp = scol[0];
+        uint32_t vp = scol[1];
+        uint32_t Rp = scol[2];
+        uint32_t Lc = scol[kHaloW];
+        uint32_t vc = scol[kHaloW + 1];
+        uint32_t Rc = scol[kHaloW + 2];
+        uint32_t hmax_p = max_pair(max_pair(Lp, vp), Rp);
+        uint32_t hmin_p = min_pair(min_pair(Lp, vp), Rp);
+        uint32_t hmax_c = max_pair(max_pair(Lc, vc), Rc);
+        uint32_t hmin_c = min_pair(min_pair(Lc, vc), Rc);
+        const int steps = min(g.th, T / 2);
+#pragma unroll 2
+        for (int t = 0; t < steps; ++t) {
+            const uint32_t* nrow = scol + (t + 2) * kHaloW;
+            const uint32_t Ln = nrow[0];
+            const uint32_t vn = nrow[1];
+            const uint32_t Rn = nrow[2];
+            const uint32_t hmax_n = max_pair(max_pair(Ln, vn), Rn);
+            const uint32_t hmin_n = min_pair(min_pair(Ln, vn), Rn);
             // 3 x 3 maxima / minima including the centre: a neighbour is
-            // greater iff the maximum of the nine is above the centre.
-            const int mx = max(max(hmax_p, hmax_c), hmax_n);
-            const unsigned mn = min(min(hmin_p, hmin_c), hmin_n);
+            // greater iff the maximum of the nine is above the centre,
+            // smaller iff the minimum is below it.
+            const uint32_t mx = max_pair(max_pair(hmax_p, hmax_c), hmax_n);
+            const uint32_t mn = min_pair(min_pair(hmin_p, hmin_c), hmin_n);
             // Lane y derives its row's listed / greater / smaller masks from
-            // these two after the scan.
-            const uint32_t bG = __ballot_sync(~0u, mx > vc);
-            const uint32_t bS = __ballot_sync(~0u, mn < static_cast<unsigned>(vc));
-            // Equalities also at columns outside the image (-1 == -1 there):
-            // every use of these masks is restricted to listed pixels.
-            const uint32_t bEU = __ballot_sync(~0u, vc == vp);
-            const uint32_t bEUL = __ballot_sync(~0u, vc == Lp);
-            const uint32_t bEUR = __ballot_sync(~0u, vc == Rp);
-            const uint32_t bEL = __ballot_sync(~0u, vc == Lc);
+            // these after the scan.  A pixel outside the image (NaN) is
+            // equal to none; every use of the equality masks is restricted
+            // to listed pixels, which are inside.
+            uint32_t bG0, bG1, bS0, bS1, bEU0, bEU1, bEUL0, bEUL1, bEUR0,
+                bEUR1, bEL0, bEL1;
+            ballot_pair_gt(mx, vc, bG0, bG1);
+            ballot_pair_lt(mn, vc, bS0, bS1);
+            ballot_pair_eq(vc, vp, bEU0, bEU1);
+            ballot_pair_eq(vc, Lp, bEUL0, bEUL1);
+            ballot_pair_eq(vc, Rp, bEUR0, bEUR1);
+            ballot_pair_eq(vc, Lc, bEL0, bEL1);
             if (lane == 0) {
-                // Row y's masks, picked up by lane y after the scan.
-                uint4* slot = reinterpret_cast<uint4*>(W + 8 * y);
-                slot[0] = make_uint4(bG, bS, bEU, bEUL);
-                slot[1] = make_uint4(bEUR, bEL, 0u, 0u);
+                // Rows t and t + 16's masks, picked up by lanes t and t + 16
+                // after the scan.
+                uint4* slot = reinterpret_cast<uint4*>(W + 8 * t);
+                slot[0] = make_uint4(bG0, bS0, bEU0, bEUL0);
+                slot[1] = make_uint4(bEUR0, bEL0, 0u, 0u);
+                uint4* slot1 = reinterpret_cast<uint4*>(W + 8 * (t + T / 2));
+                slot1[0] = make_uint4(bG1, bS1, bEU1, bEUL1);
+                slot1[1] = make_uint4(bEUR1, bEL1, 0u, 0u);
             }
             hmax_p = hmax_c;
             hmin_p = hmin_c;
@@ -500,10 +582,11 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
             Rc = Rn;
         }
         if (g.th == T) {
-            // The window now holds rows T - 1 (p) and T (c).
-            bEq[0] = __ballot_sync(~0u, vp == Lc);
-            bEq[1] = __ballot_sync(~0u, vp == vc);
-            bEq[2] = __ballot_sync(~0u, vp == Rc);
+            // The window's high halves now hold rows T - 1 (p) and T (c).
+            uint32_t lo;
+            ballot_pair_eq(vp, Lc, lo, bEq[0]);
+            ballot_pair_eq(vp, vc, lo, bEq[1]);
+            ballot_pair_eq(vp, Rc, lo, bEq[2]);
         }
     }
 
@@ -530,7 +613,9 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
 
     // Staged pixel (x, y) of the tile, x and y in -1 .. T.
     auto px = [&](int x, int y) -> int {
-        return simg[(y + 1) * kHaloW + x + 1];
+        const int r = y + 1;
+        return r < kSlotRows ? shalf[2 * (r * kHaloW + x + 1)]
+                             : shalf[2 * ((r - T / 2) * kHaloW + x + 1) + 1];
     };
 
     // -- seam masks: border pixels with an equal neighbour outside the tile --
