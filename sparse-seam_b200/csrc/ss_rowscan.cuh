@@ -17,8 +17,9 @@
 //   fragments (union-find over all fragments of the launch), or marks a live
 //   fragment whose partner across the seam is decided.
 // Flags pass: every fragment ORs its flags into its component's root.
-// Resolve pass: every logged run gets its component's verdict; runs of
-//   sparse tiles are written byte-parallel, dense tiles row by row.
+// Resolve pass: every logged run gets its component's verdict; the tile
+//   pass left its bytes at 0 in both masks, so only the bytes that become
+//   255 are written: byte-parallel for sparse tiles, word ORs for dense.
 //
 // Reference behaviour followed (paths inside the reference repository):
 // zone flags and seam test, harness/primary/snapshot_sparse_seam_cuda_v1_0.cu
@@ -309,70 +310,36 @@ struct __align__(16) ResolveSmem {
     int32_t out_pitch[32];
     int16_t tw[32];
     int16_t th[32];
-    // Per warp, one dense tile at a time: logged pixels per row, and those
-    // whose maxima / minima byte is 255.
-    Row live[kLaterWarps][TT];
+    // Per warp, one dense tile at a time: the logged pixels per row whose
+    // maxima / minima byte is 255.
     Row vmax[kLaterWarps][TT];
     Row vmin[kLaterWarps][TT];
     uint32_t flipped;         // tiles (bits of the group) with a verdict
                               //   other than their tile-local one
 };
 
-// Rewrites the logged pixels of a full tile (32 x 32, rows and origins
-// aligned to `vec` = 16, 8 or 4 bytes) from per-row bit masks: each lane
-// takes one `vec`-byte piece of a row (32 / vec lanes per row, vec rows per
-// step), loads it unless every byte is logged, replaces the logged bytes and
-// stores it back.
-__device__ __forceinline__ uint32_t merge4(uint32_t cur, uint32_t live,
-                                          uint32_t verdict) {
-    const uint32_t m = spread4(live);
-    return (cur & ~m) | (spread4(verdict) & m);
-}
-
+// Sets the mask bytes of a full tile's logged pixels whose verdict is 255
+// (rows and origin on 4-byte boundaries), from per-row bit masks: the tile
+// pass left every logged byte at 0, so ORing 0xFF into the bytes of each
+// 4-byte word that need it is the whole rewrite, one reduction per word
+// with any such byte and no read of the rows.
 template <int TT, typename Row>
-__device__ __forceinline__ void merge_rows(uint8_t* omax, uint8_t* omin,
-                                           int64_t pitch, const Row* live,
-                                           const Row* vmax, const Row* vmin,
-                                           int vec) {
+__device__ __forceinline__ void or_rows(uint8_t* omax, uint8_t* omin,
+                                        int64_t pitch, const Row* vmax,
+                                        const Row* vmin) {
     const int lane = static_cast<int>(threadIdx.x) & 31;
-    const int per_row = TT / vec;
-    const int c = lane % per_row;
-    const int rr = lane / per_row;
-    const uint32_t full = (vec == 16) ? 0xFFFFu : (vec == 8) ? 0xFFu : 0xFu;
-    for (int r0 = 0; r0 < TT; r0 += 32 / per_row) {
-        const int r = r0 + rr;
-        const uint32_t lv =
-            static_cast<uint32_t>(live[r] >> (c * vec)) & full;
-        if (lv == 0u) {
-            continue;
+    constexpr int kWords = TT / 4;   // 4-byte words per row
+    for (int i = lane; i < TT * kWords; i += 32) {
+        const int r = i / kWords;
+        const int w = i % kWords;
+        const uint32_t bx = static_cast<uint32_t>(vmax[r] >> (4 * w)) & 15u;
+        const uint32_t bn = static_cast<uint32_t>(vmin[r] >> (4 * w)) & 15u;
+        const int64_t o = static_cast<int64_t>(r) * pitch + 4 * w;
+        if (bx) {
+            atomicOr(reinterpret_cast<uint32_t*>(omax + o), spread4(bx));
         }
-        const uint32_t bx = static_cast<uint32_t>(vmax[r] >> (c * vec));
-        const uint32_t bn = static_cast<uint32_t>(vmin[r] >> (c * vec));
-        const int64_t o = static_cast<int64_t>(r) * pitch + c * vec;
-        const bool all = lv == full;
-        if (vec == 16) {
-            uint4* px = reinterpret_cast<uint4*>(omax + o);
-            uint4* pn = reinterpret_cast<uint4*>(omin + o);
-            const uint4 cx = all ? make_uint4(0u, 0u, 0u, 0u) : *px;
-            const uint4 cn = all ? make_uint4(0u, 0u, 0u, 0u) : *pn;
-            *px = make_uint4(merge4(cx.x, lv, bx), merge4(cx.y, lv >> 4, bx >> 4),
-                             merge4(cx.z, lv >> 8, bx >> 8),
-                             merge4(cx.w, lv >> 12, bx >> 12));
-            *pn = make_uint4(merge4(cn.x, lv, bn), merge4(cn.y, lv >> 4, bn >> 4),
-                             merge4(cn.z, lv >> 8, bn >> 8),
-                             merge4(cn.w, lv >> 12, bn >> 12));
-        } else if (vec == 8) {
-            uint2* px = reinterpret_cast<uint2*>(omax + o);
-            uint2* pn = reinterpret_cast<uint2*>(omin + o);
-            const uint2 cx = all ? make_uint2(0u, 0u) : *px;
-            const uint2 cn = all ? make_uint2(0u, 0u) : *pn;
-            *px = make_uint2(merge4(cx.x, lv, bx), merge4(cx.y, lv >> 4, bx >> 4));
-            *pn = make_uint2(merge4(cn.x, lv, bn), merge4(cn.y, lv >> 4, bn >> 4));
-        } else {
-            uint32_t* px = reinterpret_cast<uint32_t*>(omax + o);
-            uint32_t* pn = reinterpret_cast<uint32_t*>(omin + o);
-            *px = merge4(all ? 0u : *px, lv, bx);
-            *pn = merge4(all ? 0u : *pn, lv, bn);
+        if (bn) {
+            atomicOr(reinterpret_cast<uint32_t*>(omin + o), spread4(bn));
         }
     }
 }
@@ -487,17 +454,21 @@ __device__ __forceinline__ void resolve_group(ResolveSmem<TT>& sm,
             const int64_t o = __shfl_sync(~0u, off, src_lane) +
                               (bi - __shfl_sync(~0u, excl_len, src_lane));
             const uint32_t vd = __shfl_sync(~0u, verdict, src_lane);
+            // The tile pass left both bytes at 0: only a 255 is written.
             if (bi < bytes) {
-                sm.maxima[tile_of][o] = static_cast<uint8_t>(vd);
-                sm.minima[tile_of][o] = static_cast<uint8_t>(vd >> 8);
+                if (vd & 0xFFu) {
+                    sm.maxima[tile_of][o] = 0xFF;
+                }
+                if (vd & 0xFF00u) {
+                    sm.minima[tile_of][o] = 0xFF;
+                }
             }
         }
     }
     // Tiles with many logged runs, dealt out to the warps one tile at a
-    // time: their pixels and verdicts as row masks, then the tile's rows
-    // rewritten (logged bytes replaced, the others kept).
+    // time: the pixels whose maxima / minima byte becomes 255 as row masks,
+    // then those bytes set.
     const uint32_t dense = __ballot_sync(~0u, n > kSparseRuns);
-    Row* live_rows = sm.live[warp];
     Row* vmax_rows = sm.vmax[warp];
     Row* vmin_rows = sm.vmin[warp];
     int rank = 0;
@@ -509,7 +480,6 @@ __device__ __forceinline__ void resolve_group(ResolveSmem<TT>& sm,
         const uint32_t nt = __shfl_sync(~0u, n, t);
         const uint32_t kt = __shfl_sync(~0u, k, t);
         for (int r = lane; r < TT; r += 32) {
-            live_rows[r] = 0u;
             vmax_rows[r] = 0u;
             vmin_rows[r] = 0u;
         }
@@ -533,7 +503,6 @@ __device__ __forceinline__ void resolve_group(ResolveSmem<TT>& sm,
             }
             const Row R = ((Row(2) << (x + n_px - 1)) - Row(1)) &
                           ~((Row(1) << x) - Row(1));
-            atomicOr(&live_rows[y], R);
             if (!(fl & kHasGreater)) {
                 atomicOr(&vmax_rows[y], R);
             }
@@ -548,21 +517,19 @@ __device__ __forceinline__ void resolve_group(ResolveSmem<TT>& sm,
         const uint64_t align = reinterpret_cast<uint64_t>(omax) |
                                reinterpret_cast<uint64_t>(omin) |
                                static_cast<uint64_t>(pitch);
-        int vec = (align & 15u) == 0 ? 16 : (align & 7u) == 0 ? 8
-                : (align & 3u) == 0 ? 4 : 1;
-        if (tw < TT || th < TT) {
-            vec = 1;
-        }
-        if (vec > 1) {
-            merge_rows<TT>(omax, omin, pitch, live_rows, vmax_rows, vmin_rows,
-                           vec);
+        // Whole 4-byte words only inside a full tile: a partial tile's last
+        // word may reach past the image's row (and buffer) end.
+        if ((align & 3u) == 0 && tw == TT && th == TT) {
+            or_rows<TT>(omax, omin, pitch, vmax_rows, vmin_rows);
         } else {
             for (int r = 0; r < th; ++r) {
                 for (int x = lane; x < TT; x += 32) {
-                    if ((live_rows[r] >> x) & 1u) {
-                        const int64_t o = static_cast<int64_t>(r) * pitch + x;
-                        omax[o] = ((vmax_rows[r] >> x) & 1u) ? 255 : 0;
-                        omin[o] = ((vmin_rows[r] >> x) & 1u) ? 255 : 0;
+                    const int64_t o = static_cast<int64_t>(r) * pitch + x;
+                    if ((vmax_rows[r] >> x) & 1u) {
+                        omax[o] = 255;
+                    }
+                    if ((vmin_rows[r] >> x) & 1u) {
+                        omin[o] = 255;
                     }
                 }
             }
