@@ -214,8 +214,16 @@ __device__ __forceinline__ void seam_pass_group(const Source& src,
                     fo = static_cast<int>(g * kSlots + rec);
                     target = -1;
                 } else if (rn < static_cast<uint32_t>(kSlots)) {
-                    fo = static_cast<int>(g * kSlots + rec);
-                    target = static_cast<int>(ng * kSlots + rn);
+                    // Both pixels live: the neighbour tile holds the mirror
+                    // item (its pixel is live and equal to this one, and its
+                    // streaks keep at least one pair per zone pair and
+                    // direction, as this tile's do), so only the items facing
+                    // a later tile (right, bottom and the bottom corners)
+                    // link; the others would repeat the same unions.
+                    if (dir >= kRelRight) {
+                        fo = static_cast<int>(g * kSlots + rec);
+                        target = static_cast<int>(ng * kSlots + rn);
+                    }
                 } else {
                     err = kErrInvariant;   // equal across a seam, no seam zone
                 }
