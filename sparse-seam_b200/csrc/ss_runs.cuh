@@ -624,8 +624,9 @@ __device__ __forceinline__ void tile_pass_runs(uint32_t* words, RunAux& ax,
     // masks against the halo row (up-left, up, up-right); bottom: the
     // scan's last step; left: bits 0 of the rows' up-left / left masks and
     // one comparison with the halo pixel below-left; right: bits 31 of the
-    // up-right masks and two comparisons with the halo column.  Equalities
-    // between two pixels outside the image hold, so every use is restricted
+    // up-right masks and two comparisons with the halo column.  An equality
+    // that involves a pixel outside the image means nothing (false in the
+    // scan's masks, staged bits compared here), so every use is restricted
     // to listed pixels.
     uint32_t sT, sB, sLc, sRc;
     {
