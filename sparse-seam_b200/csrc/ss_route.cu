@@ -442,6 +442,19 @@ __global__ void empty_kernel() {}
 // each; T = 64: four quadrant warps per tile), seam, flags, resolve passes.
 // ---------------------------------------------------------------------------
 
+// Programmatic dependent launch between the row-scan passes.  Each pass
+// lets the next one's CTAs be launched once all of its own CTAs have
+// started (they then take SM slots as this pass's last CTAs leave, instead
+// of after the launch gap), and a pass launched that way waits, before any
+// work, until its predecessor grid has completed and its writes are
+// visible.  In a kernel launched without the attribute both are no-ops.
+__device__ __forceinline__ void allow_next_pass() {
+    asm volatile("griddepcontrol.launch_dependents;" :::);
+}
+__device__ __forceinline__ void wait_previous_pass() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // Row-scan tile pass: NW independent warps per CTA, one tile each; at most
 // 64 registers per thread, so 32 warps fit on an SM (the shared-memory
 // limit at 6.6 KB per warp).  The persistent form gets the same budget: at
@@ -450,6 +463,7 @@ template <int NW, bool kPersistent>
 __global__ void __launch_bounds__(NW * 32, 32 / NW)
 runs_tile_pass_kernel(Source src, Arena a) {
     __shared__ rowscan::RunSmem sm[NW];
+    allow_next_pass();
     const int warp = static_cast<int>(threadIdx.x) >> 5;
     const int lane = static_cast<int>(threadIdx.x) & 31;
     if (a.header->magic != kMagic) {
@@ -499,6 +513,7 @@ runs64_tile_pass_kernel(Source src, Arena a) {
     __shared__ rowscan::RunSmem64 sm;
     __shared__ uint32_t next_item;
     const int warp = static_cast<int>(threadIdx.x) >> 5;
+    allow_next_pass();
     if (a.header->magic != kMagic) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             raise_error(a.header, kErrUninitialized, 0u);
@@ -536,6 +551,8 @@ runs64_tile_pass_kernel(Source src, Arena a) {
 template <int TT>
 __global__ void __launch_bounds__(rowscan::kLaterWarps * 32)
 rowscan_seam_pass_kernel(Source src, Arena a) {
+    wait_previous_pass();
+    allow_next_pass();
     if (a.header->magic != kMagic) {
         return;
     }
@@ -550,6 +567,8 @@ rowscan_seam_pass_kernel(Source src, Arena a) {
 template <int TT>
 __global__ void __launch_bounds__(rowscan::kLaterWarps * 32)
 rowscan_flags_pass_kernel(Source src, Arena a) {
+    wait_previous_pass();
+    allow_next_pass();
     if (a.header->magic != kMagic) {
         return;
     }
@@ -567,6 +586,7 @@ rowscan_resolve_pass_kernel(Source src, Arena a) {
     __shared__ rowscan::ResolveSmem<TT> sm;
     __shared__ uint32_t next_group;
     const int warp = static_cast<int>(threadIdx.x) >> 5;
+    wait_previous_pass();
     if (a.header->magic != kMagic) {
         return;
     }
@@ -850,6 +870,24 @@ bool workspace_bytes_for_tiles(int64_t tiles, int tile, size_t* bytes) {
     return tile_ok(tile) && tiles >= 0 && workspace_size(tiles, tile, bytes);
 }
 
+// Launches a pass after the row-scan tile pass, allowed to start before its
+// predecessor ends (it waits for it on the device).
+static void launch_next_pass(Kernel k, unsigned grid, unsigned threads,
+                             cudaStream_t stream, const Source& src,
+                             const Arena& arena) {
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(grid);
+    lc.blockDim = dim3(threads);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    (void)cudaLaunchKernelEx(&lc, k, src, arena);
+}
+
 static ss_status launch_route(const Config& cfg, const Source& src_in,
                               const Arena& arena, int persistent,
                               cudaStream_t stream, int passes = 7,
@@ -894,22 +932,29 @@ static ss_status launch_route(const Config& cfg, const Source& src_in,
         cfg.tile_pass[p]<<<grid1, threads, 0, stream>>>(src, arena);
     }
     if ((passes & 4) && cfg.seam_pass) {
-        cfg.seam_pass<<<static_cast<unsigned>(ctas2), later_threads, 0,
-                        stream>>>(src, arena);
+        launch_next_pass(cfg.seam_pass, static_cast<unsigned>(ctas2),
+                         later_threads, stream, src, arena);
         if (cfg.flags_pass) {
             src.flatten = flatten;
             if (flatten == kFlattenSeparate) {
                 Source only = src;
                 only.flatten = kFlattenOnly;
-                cfg.flags_pass<<<static_cast<unsigned>(ctas2), later_threads,
-                                 0, stream>>>(only, arena);
+                launch_next_pass(cfg.flags_pass, static_cast<unsigned>(ctas2),
+                                 later_threads, stream, only, arena);
             }
-            cfg.flags_pass<<<static_cast<unsigned>(ctas2), later_threads, 0,
-                             stream>>>(src, arena);
+            launch_next_pass(cfg.flags_pass, static_cast<unsigned>(ctas2),
+                             later_threads, stream, src, arena);
         }
     }
     if (passes & 2) {
-        cfg.resolve_pass[p]<<<grid2, later_threads, 0, stream>>>(src, arena);
+        if (cfg.seam_pass) {
+            // Row-scan resolve pass: waits for its predecessor on the device.
+            launch_next_pass(cfg.resolve_pass[p], grid2, later_threads,
+                             stream, src, arena);
+        } else {
+            cfg.resolve_pass[p]<<<grid2, later_threads, 0, stream>>>(src,
+                                                                     arena);
+        }
     }
     return cudaGetLastError() == cudaSuccess ? SS_OK : SS_ERR_CUDA;
 }
