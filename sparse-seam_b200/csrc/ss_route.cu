@@ -1357,9 +1357,17 @@ static ss_status batch_passes(const void* h_plan, const void* d_plan,
     }
     const PlanHeader* dph = static_cast<const PlanHeader*>(d_plan);
     Source src{};
-    src.images = reinterpret_cast<const PlanImage*>(dph + 1);
-    src.tile_image =
-        reinterpret_cast<const int32_t*>(src.images + ph->count);
+    if (ph->count == 1) {
+        // One image: its entry travels in the launch parameters, as for a
+        // single call, instead of being looked up per tile.
+        src.images = nullptr;
+        src.tile_image = nullptr;
+        src.single = *reinterpret_cast<const PlanImage*>(ph + 1);
+    } else {
+        src.images = reinterpret_cast<const PlanImage*>(dph + 1);
+        src.tile_image =
+            reinterpret_cast<const int32_t*>(src.images + ph->count);
+    }
     src.total_tiles = ph->total_tiles;
     return launch_route(*cfg, src, arena_at(d_workspace, L),
                         persistent ? 1 : 0,
