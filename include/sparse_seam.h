@@ -130,7 +130,7 @@ typedef struct ss_stats {
  *   warps < 0   row-scan kernels (per-row bit masks and runs): tile 32, one
  *               tile per warp, -warps warps per CTA (2 or 4); tile 64 (-4),
  *               one tile per CTA of four warps, one per 32 x 32 quadrant
- * Defaults: tile 16 -> 4, tile 32 -> -2, tile 64 -> -4.  The reference fixes
+ * Defaults: tile 16 -> 4, tile 32 -> -4, tile 64 -> -4.  The reference fixes
  * its tile and classify threads at compile time
  * (harness/configuration_study/sparse_config_benchmark_v0_8.cu:17-30). */
 ss_status ss_set_kernel_config(int tile, int warps);

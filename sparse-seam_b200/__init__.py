@@ -267,7 +267,7 @@ def get_kernel_config(tile: int) -> int:
     return int(out.value)
 
 
-KERNEL_CONFIGS = {16: (2, 4, 8), 32: (-2, -4, 4, 8, 16), 64: (-4, 8, 16)}
+KERNEL_CONFIGS = {16: (4, 2, 8), 32: (-4, -2, 4, 8, 16), 64: (-4, 8, 16)}
 
 
 def workspace_bytes(width: int, height: int, tile: int = 32) -> int:

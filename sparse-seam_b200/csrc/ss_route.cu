@@ -784,7 +784,7 @@ static const Config kConfigs[] = {
 
 // Per tile size, the configuration used by default (index by tile / 16 - 1);
 // negative warps select the row-scan kernels.
-static std::atomic<int> g_default_warps[4] = {{4}, {-2}, {0}, {-4}};
+static std::atomic<int> g_default_warps[4] = {{4}, {-4}, {0}, {-4}};
 
 static const Config* find_config(int tile, int warps) {
     for (const Config& c : kConfigs) {
