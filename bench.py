@@ -79,6 +79,12 @@ def parse_args():
                    help="re-quantise the corpus to this many gray levels")
     p.add_argument("--sweep", action="store_true",
                    help="add the quantisation x tile sweep of the corpus")
+    p.add_argument("--schedule", default="auto",
+                   choices=["auto", "grid", "persistent"],
+                   help="tile-pass schedule of the timed steps: the faster "
+                        "of the two in a short probe (default), or pinned "
+                        "(for profiling, where the probe's timings are the "
+                        "profiler's)")
     p.add_argument("--serve-seconds", type=float, default=60.0,
                    help="duration of each Poisson rate of the served stream")
     return p.parse_args()
@@ -544,7 +550,8 @@ def main():
         timed(lambda: plan.run(ws, persistent=persistent, stream=stream), 2)
         sched[persistent] = timed(
             lambda: plan.run(ws, persistent=persistent, stream=stream), 3)
-    persistent = sched[True] < sched[False]
+    persistent = (sched[True] < sched[False] if args.schedule == "auto"
+                  else args.schedule == "persistent")
     ws.read_status(stream)
 
     launches_per_run = 4 if pkg.get_kernel_config(tile) < 0 else 2
@@ -614,7 +621,7 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u8", "data": "synthetic (seeded smooth-noise corpus)",
         "config": config_dict(args),
-        "schedule": {"persistent": persistent,
+        "schedule": {"persistent": persistent, "choice": args.schedule,
                      "ms_grid": round(sched[False], 4),
                      "ms_persistent": round(sched[True], 4)},
         "gpu_launches": launches_per_run * args.steps,
