@@ -563,8 +563,9 @@ def main():
         stream.synchronize()
         with torch.cuda.graph(graph, stream=stream):
             plan.run(ws, persistent=persistent, stream=stream)
-    for _ in range(args.warmup):
-        graph.replay()
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            graph.replay()
     stream.synchronize()
     dist.barrier()
     torch.cuda.synchronize()
@@ -787,9 +788,13 @@ def secondary(args, pkg, plan, images, host_images, maxs, mins, stream, dist,
                 for i in sel:
                     pkg.extrema(images[i], tile, maxs[i], mins[i], ws1,
                                 stream=stream)
-        for _ in range(args.warmup):
-            g.replay()
-        stream.synchronize()
+        # Warm-up replays on the timing stream, and the device drained: a
+        # replay left running on another stream would fall inside the timed
+        # window.
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                g.replay()
+        torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
@@ -1016,9 +1021,12 @@ def _graph_ms(fn, stream, warmup: int, reps: int) -> float:
         stream.synchronize()
         with torch.cuda.graph(g, stream=stream):
             fn()
-    for _ in range(max(1, warmup)):
-        g.replay()
-    stream.synchronize()
+    # Warm-up replays on the timing stream, and the device drained: a replay
+    # left running on another stream would fall inside the timed window.
+    with torch.cuda.stream(stream):
+        for _ in range(max(1, warmup)):
+            g.replay()
+    torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
