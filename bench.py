@@ -910,20 +910,23 @@ def _later_group(tiles: int, sms: int) -> int:
 
 def launch_floor_section(pkg, device, stream, n_images, warmup, reps):
     """Graph replay of 1 and of 4 empty kernels per 2040x1356 image, with the
-    grid shapes of the route's tile pass (2 warps per CTA, one tile per warp)
-    and later passes (8 warps per CTA): the floor no launch-based per-image
-    route goes below."""
+    grid shapes of the route's tile pass (the default row-scan CTAs, one tile
+    per warp) and later passes (8 warps per CTA): the floor no launch-based
+    per-image route goes below."""
     import torch
     lib = pkg.lib()
     sms = torch.cuda.get_device_properties(device).multi_processor_count
     tiles = ((2040 + 31) // 32) * ((1356 + 31) // 32)
-    g1 = (tiles + 1) // 2
+    cfg = pkg.get_kernel_config(32)
+    warps = abs(cfg)
+    per_cta = warps if cfg < 0 else 1     # row-scan: a tile per warp
+    g1 = (tiles + per_cta - 1) // per_cta
     g2 = (tiles + _later_group(tiles, sms) - 1) // _later_group(tiles, sms)
 
     def run(k):
         s = ctypes.c_void_p(stream.cuda_stream)
         for _ in range(n_images):
-            assert lib.ss_empty_launches(1, g1, 64, s) == 0
+            assert lib.ss_empty_launches(1, g1, 32 * warps, s) == 0
             if k > 1:
                 assert lib.ss_empty_launches(k - 1, g2, 256, s) == 0
 
