@@ -178,6 +178,43 @@ class HostBatch:
         start_stream.wait_event(end)
         return end
 
+    def tune_threads(self, stream=None, candidates=None, reps: int = 3) -> int:
+        """Picks the host thread count of the mask expansion by timing.
+
+        The expansion shares the host's memory with the copy engines' reads
+        of the inputs, and how many threads pay off depends on the host and
+        on what else runs there.  Times `reps` passes per candidate (by
+        default a quarter, half and all but one of the processors), keeps the
+        fastest in `self.threads` and returns it.
+        """
+        import os
+        import torch
+        if not self.packed:
+            return self.threads
+        if candidates is None:
+            try:
+                procs = len(os.sched_getaffinity(0))
+            except AttributeError:
+                procs = os.cpu_count() or 1
+            candidates = sorted({max(1, procs // 4), max(1, procs // 2),
+                                 max(1, procs - 1)})
+        stream = stream or torch.cuda.current_stream(self.device)
+        best, best_ms = self.threads, None
+        for t in candidates:
+            self.threads = int(t)
+            self.run(stream)                      # settle at this count
+            start = torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            end = None
+            for _ in range(reps):
+                end = self.run(stream)
+            end.synchronize()
+            ms = start.elapsed_time(end) / reps
+            if best_ms is None or ms < best_ms:
+                best, best_ms = int(t), ms
+        self.threads = best
+        return best
+
     def check(self) -> None:
         """Synchronises and raises on a device-side failure."""
         import torch

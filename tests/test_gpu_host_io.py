@@ -54,3 +54,23 @@ def test_host_batch_matches_oracle(packed):
             assert np.array_equal(hb.minima[i], want[1]), (packed, rep, i)
     if packed:
         assert hb.d2h_bytes < hb.pixels // 3
+
+
+def test_host_batch_thread_tuning_keeps_masks():
+    """tune_threads picks one of the candidates by timing; passes at the
+    picked count still give the oracle's masks."""
+    host = importlib.import_module("sparse-seam_b200.host")
+    synth = importlib.import_module("sparse-seam_b200.synth")
+    images = [t.cpu().numpy() for t in
+              synth.uneven_batch(12, seed=5, lo=40, hi=500)]
+    hb = host.HostBatch(images, tile=32, chunks=3, packed=True)
+    picked = hb.tune_threads(candidates=(1, 2, 3), reps=1)
+    assert picked in (1, 2, 3) and hb.threads == picked
+    for m in hb.maxima + hb.minima:
+        m[...] = 7
+    hb.run().synchronize()
+    hb.check()
+    for i, im in enumerate(images):
+        want = oracle.extrema(im)
+        assert np.array_equal(hb.maxima[i], want[0]), i
+        assert np.array_equal(hb.minima[i], want[1]), i
