@@ -62,6 +62,10 @@ def parse_args():
     p.add_argument("--impl", default="sparse-seam-b200",
                    choices=["sparse-seam-b200", "reference"])
     p.add_argument("--tile", type=int, default=32)
+    p.add_argument("--warps", type=int, default=0,
+                   help="kernel family for --tile (ss_set_kernel_config: "
+                        "< 0 row-scan, > 0 CTA-per-tile warps; 0 = the "
+                        "library's default)")
     p.add_argument("--large", type=int, default=100)
     p.add_argument("--small", type=int, default=100)
     p.add_argument("--quick", action="store_true",
@@ -402,6 +406,7 @@ def config_dict(args):
                      f"{args.small} x 481x321 uint8 smooth noise, "
                      f"{args.levels} levels"),
         "tile": args.tile,
+        "kernel_config": args.warps or "default",
         "images_per_step": args.large + args.small,
         "pixels_per_step": sum(h * w for h, w in
                                corpus_shapes(args.large, args.small)),
@@ -487,6 +492,8 @@ def main():
     device = torch.device("cuda", dist.local)
     torch.cuda.set_device(device)
     tile = args.tile
+    if args.warps:
+        pkg.set_kernel_config(tile, args.warps)
 
     images = make_corpus(args.large, args.small, corpus_seed_base(dist.rank),
                          device, args.levels)
