@@ -229,8 +229,10 @@ ss_status ss_batch_plan_fill(const ss_image_desc* descs, int count, int tile,
                              size_t* workspace_bytes);
 
 /* Enqueues the route over every image of a plan.  `h_plan` is the host plan
- * filled by ss_batch_plan_fill (read for sizes only), `d_plan` its device
- * copy (read by the kernels).  Each image gets its own seam-fragment arena
+ * filled by ss_batch_plan_fill (read for sizes, and for the image entry of
+ * a one-image plan, which travels in the launch parameters), `d_plan` its
+ * device copy (read by the kernels); the two must hold the same bytes when
+ * the call is made (or captured).  Each image gets its own seam-fragment arena
  * inside the workspace; results are the same as calling ss_extrema on each
  * image alone.
  *   persistent  0: one CTA per (image, tile) work item;

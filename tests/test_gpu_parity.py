@@ -321,3 +321,31 @@ def test_seam_statistics(tile):
     assert st.live_pixels == sum(p.live_pixels for p in per)
     assert st.active_fragments == sum(p.active_fragments for p in per)
     assert st.tiles == sum(p.tiles for p in per)
+
+
+@pytest.mark.parametrize("tile", [16, 32, 64])
+@pytest.mark.parametrize("persistent", [False, True])
+def test_one_image_plans_match_the_oracle(tile, persistent):
+    """A one-image plan carries its image in the launch parameters (no
+    per-tile lookup); its masks equal the oracle's, with and without the
+    persistent queue, at every tile edge, and with re-quantisation."""
+    import importlib
+    pkg = package()
+    synth = importlib.import_module("sparse-seam_b200.synth")
+    for seed, (h, w) in enumerate([(1, 1), (37, 300), (301, 203)]):
+        im = synth.smooth_noise(h, w, seed, device="cuda")
+        for levels in (256, 5):
+            mx, mn = torch.empty_like(im), torch.empty_like(im)
+            plan = pkg.BatchPlan([im], [mx], [mn], tile=tile, levels=levels)
+            ws = plan.make_workspace()
+            for _ in range(2):   # the persistent queue rewinds between runs
+                plan.run(ws, persistent=persistent)
+            ws.read_status()
+            host = im.cpu().numpy()
+            if levels < 256:
+                b = (host.astype(np.int32) * levels) >> 8
+                host = ((b * 255 + (levels - 1) // 2) //
+                        (levels - 1)).astype(np.uint8)
+            assert_same((mx.cpu().numpy(), mn.cpu().numpy()),
+                        oracle.extrema(host),
+                        f"one-image plan {h}x{w} T={tile} L={levels}")
