@@ -333,7 +333,8 @@ def test_one_image_plans_match_the_oracle(tile, persistent):
     pkg = package()
     synth = importlib.import_module("sparse-seam_b200.synth")
     for seed, (h, w) in enumerate([(1, 1), (37, 300), (301, 203)]):
-        im = synth.smooth_noise(h, w, seed, device="cuda")
+        im = (synth.smooth_noise(h, w, seed, device="cuda") if h * w > 1 else
+              torch.full((h, w), 9, dtype=torch.uint8, device="cuda"))
         for levels in (256, 5):
             mx, mn = torch.empty_like(im), torch.empty_like(im)
             plan = pkg.BatchPlan([im], [mx], [mn], tile=tile, levels=levels)
